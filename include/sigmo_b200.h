@@ -1,0 +1,241 @@
+/*
+ * sigmo_b200 — C ABI of the B200-native SIGMo hot path.
+ *
+ * The reference (SIGMo, a header-only C++20/SYCL library) exposes no FFI; its
+ * boundary is the C++ API that library/src/sigmo.cpp calls.  Every entry point
+ * below replaces one of those calls (file:line cited beside it).  Handles are
+ * opaque; every function returns a status (SIGMO_OK == 0) and leaves a
+ * thread-local message for sigmo_last_error().  No torch types appear here.
+ *
+ * Semantics profiles.  The reference's hot path contains shift counts that
+ * reach the register width and a bitset indexed through uint8_t; its results
+ * on the NVIDIA PTX target it was written for are the parity contract:
+ *   SIGMO_PROFILE_REF_PTX  (default) shift count >= width yields 0
+ *   SIGMO_PROFILE_EXACT    exact sets, correct range masks, injective DFS
+ *   SIGMO_PROFILE_REF_X86  accepted only by the CPU oracle (not this library)
+ */
+#ifndef SIGMO_B200_H
+#define SIGMO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SIGMO_API __attribute__((visibility("default")))
+#else
+#define SIGMO_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  SIGMO_OK = 0,
+  SIGMO_ERR_INVALID = 1,     /* bad argument / handle / size mismatch        */
+  SIGMO_ERR_CUDA = 2,        /* a CUDA runtime call failed                   */
+  SIGMO_ERR_OOM = 3,         /* device or host allocation failed             */
+  SIGMO_ERR_DOMAIN = 4,      /* input outside the supported domain           */
+  SIGMO_ERR_FORMAT = 5,      /* malformed graph text ("Invalid graph format") */
+  SIGMO_ERR_NO_DEVICE = 6,   /* no CUDA device / device index out of range    */
+  SIGMO_ERR_TIMEOUT = 7      /* a bounded device-side wait ran out            */
+};
+
+enum { SIGMO_PROFILE_REF_PTX = 0, SIGMO_PROFILE_REF_X86 = 1, SIGMO_PROFILE_EXACT = 2 };
+
+/* SignatureScope (library/include/signature.hpp:18) */
+enum { SIGMO_SCOPE_DATA = 0, SIGMO_SCOPE_QUERY = 1 };
+
+/* Message of the last failing call on this thread ("" if none). */
+SIGMO_API const char* sigmo_last_error(void);
+/* Library version string. */
+SIGMO_API const char* sigmo_version(void);
+
+/* ---- host graphs: io + batching --------------------------------------- */
+/* Batched CSR with global vertex ids — the arrays createDeviceCSRGraph builds
+ * on the host (library/include/graph.hpp:255-294).  Memory owned by the
+ * library when produced by sigmo_parse_graphs / sigmo_generate_*; free with
+ * sigmo_host_graphs_free. */
+typedef struct sigmo_host_graphs {
+  uint32_t num_graphs;
+  uint64_t total_nodes;
+  uint64_t total_edges;      /* directed CSR entries (2 x undirected edges) */
+  uint32_t* graph_offsets;   /* [num_graphs + 1]  first global vertex of g  */
+  uint32_t* row_offsets;     /* [total_nodes + 1] global CSR row pointers   */
+  uint32_t* column_indices;  /* [total_edges]     global neighbour ids      */
+  uint8_t* node_labels;      /* [total_nodes]                               */
+  uint8_t* edge_labels;      /* [total_edges]                               */
+} sigmo_host_graphs;
+
+/* io::loadCSRGraphsFromLines + createDeviceCSRGraph's host concatenation
+ * (library/include/io.hpp:46-55, graph.hpp:154-247, 255-294): one graph per
+ * line in the "n#N l#L (id label)xN e#E (u v [label])xE" format; empty lines
+ * are skipped.  SIGMO_ERR_FORMAT on a malformed line. */
+SIGMO_API int sigmo_parse_graphs(const char* text, size_t len, sigmo_host_graphs* out);
+/* Concatenation of already-batched sets (graph order kept; ids re-based). */
+SIGMO_API int sigmo_host_graphs_concat(const sigmo_host_graphs* a, const sigmo_host_graphs* b, sigmo_host_graphs* out);
+/* Graphs [first, first+count) of a batch as a new batch (ids re-based to 0). */
+SIGMO_API int sigmo_host_graphs_slice(const sigmo_host_graphs* in, uint32_t first, uint32_t count, sigmo_host_graphs* out);
+/* Write a batch back in the text format (buffer sized by a first call with
+ * buf == NULL; *len receives the byte count). */
+SIGMO_API int sigmo_format_graphs(const sigmo_host_graphs* in, char* buf, size_t* len);
+SIGMO_API void sigmo_host_graphs_free(sigmo_host_graphs* g);
+
+/* ---- seeded synthetic inputs (stand-ins for the missing ZINC / SMARTS sets) */
+/* kind: 0 = drug-like molecules (sizes uniform in [min_atoms, max_atoms]),
+ *       1 = heavy-tailed lognormal sizes (median `median`, clipped to
+ *           [min_atoms, max_atoms]) with 5% macrocycles / fused ring systems,
+ *       2 = ring-rich molecules (2-6 fused aromatic 6-cycles, carbon chains
+ *           up to 20 atoms).
+ * Vertex labels use the reference's encoding (scripts/smile2graph.py:13:
+ * N=0 Cl=1 *=2 Br=3 I=4 P=5 H=6 O=7 C=8 S=9 F=10); bond labels single=1
+ * double=2 triple=3 aromatic=4 (scripts/smile2graph.py:14). */
+SIGMO_API int sigmo_generate_molecules(int kind, uint32_t count, uint32_t min_atoms, uint32_t max_atoms, double median,
+                             uint64_t seed, sigmo_host_graphs* out);
+/* Queries: connected induced subgraphs of freshly seeded molecules (kind as
+ * above), sizes in [min_atoms, max_atoms]; skew_lo/skew_hi > 0 skews 70% of
+ * the sizes into [skew_lo, skew_hi].  kind 3 = highly automorphic patterns
+ * (6-cycles, fused bi/tri-cycles, carbon chains, branched carbon stars). */
+SIGMO_API int sigmo_generate_queries(int kind, uint32_t count, uint32_t min_atoms, uint32_t max_atoms, uint32_t skew_lo,
+                           uint32_t skew_hi, uint64_t seed, sigmo_host_graphs* out);
+
+/* ---- queue: replaces sycl::queue + device::DeviceOptions ---------------- */
+typedef struct sigmo_queue_s* sigmo_queue_t;
+
+typedef struct sigmo_options {
+  int profile;                    /* SIGMO_PROFILE_*                          */
+  uint32_t join_work_group_size;  /* DeviceOptions, device.hpp:17-21 (128)   */
+  uint32_t filter_work_group_size;/* (512) accepted for API parity           */
+} sigmo_options;
+
+SIGMO_API void sigmo_default_options(sigmo_options* o);
+/* sycl::queue{gpu_selector_v, enable_profiling} (library/src/sigmo.cpp:19). */
+SIGMO_API int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out);
+SIGMO_API int sigmo_queue_destroy(sigmo_queue_t q);
+/* queue.wait_and_throw() (sigmo.cpp:103 and after every stage). */
+SIGMO_API int sigmo_queue_wait(sigmo_queue_t q);
+/* The queue's cudaStream_t (as void*), for callers that order work with it. */
+SIGMO_API int sigmo_queue_stream(sigmo_queue_t q, void** stream);
+/* BatchedEvent::getProfilingInfo (library/include/utils.hpp:149-157): device
+ * time of the last stage launched on the queue, after it has completed. */
+SIGMO_API int sigmo_queue_last_stage_ms(sigmo_queue_t q, double* ms);
+/* Device memory: global_mem_size (sigmo.cpp:20) and name (sigmo.cpp:21). */
+SIGMO_API int sigmo_queue_device_info(sigmo_queue_t q, uint64_t* global_mem, char* name, size_t name_len);
+/* Kernels launched by this library on this queue since creation. */
+SIGMO_API int sigmo_queue_launch_count(sigmo_queue_t q, uint64_t* launches);
+
+/* ---- device batched CSR graph (DeviceBatchedCSRGraph, graph.hpp:62-112) -- */
+typedef struct sigmo_graph_s* sigmo_graph_t;
+
+/* createDeviceCSRGraph (graph.hpp:255-314): copies the batch to the device. */
+SIGMO_API int sigmo_graph_create(sigmo_queue_t q, const sigmo_host_graphs* host, sigmo_graph_t* out);
+/* Same, but the five arrays are already device-resident (no copy; the caller
+ * keeps ownership and must keep them alive). */
+SIGMO_API int sigmo_graph_create_device(sigmo_queue_t q, uint32_t num_graphs, uint64_t total_nodes, uint64_t total_edges,
+                              const uint32_t* d_graph_offsets, const uint32_t* d_row_offsets,
+                              const uint32_t* d_column_indices, const uint8_t* d_node_labels,
+                              const uint8_t* d_edge_labels, sigmo_graph_t* out);
+/* destroyDeviceCSRGraph (graph.hpp:316-322). */
+SIGMO_API int sigmo_graph_destroy(sigmo_graph_t g);
+SIGMO_API int sigmo_graph_info(sigmo_graph_t g, uint32_t* num_graphs, uint64_t* total_nodes, uint64_t* total_edges,
+                     uint32_t* max_graph_nodes);
+/* getDeviceGraphAllocSize (graph.hpp:324-328, 423-432). */
+SIGMO_API int sigmo_graph_alloc_size(sigmo_graph_t g, uint64_t* bytes);
+
+/* ---- candidate bitsets (candidates::Candidates, candidates.hpp:14-204) ---- */
+typedef struct sigmo_candidates_s* sigmo_candidates_t;
+
+/* Candidates(queue, source_nodes, target_nodes): zero-filled bit matrix
+ * (candidates.hpp:165-179).  Rows are padded on the device to a multiple of
+ * 32 words (128 B); the host view is the reference's dense [source][W]. */
+SIGMO_API int sigmo_candidates_create(sigmo_queue_t q, uint64_t source_nodes, uint64_t target_nodes, sigmo_candidates_t* out);
+SIGMO_API int sigmo_candidates_destroy(sigmo_candidates_t c);
+/* Words per row in the reference layout: ceil(target_nodes / 32). */
+SIGMO_API int sigmo_candidates_words_per_row(sigmo_candidates_t c, uint64_t* words);
+/* getAllocationSize (candidates.hpp:196): bytes of the reference layout. */
+SIGMO_API int sigmo_candidates_alloc_size(sigmo_candidates_t c, uint64_t* bytes);
+/* getHostCandidates (candidates.hpp:185-190): rows [row0, row0+rows) into
+ * host memory, dense [rows][W] uint32. */
+SIGMO_API int sigmo_candidates_download(sigmo_candidates_t c, uint64_t row0, uint64_t rows, uint32_t* host);
+/* Per-row candidate counts (getCandidatesCount(source), candidates.hpp:77-81)
+ * computed on the device; host array of source_nodes entries. */
+SIGMO_API int sigmo_candidates_row_counts(sigmo_candidates_t c, uint32_t* host_counts);
+/* XOR/rotate digest of every row (order-sensitive), for checks at sizes whose
+ * bitset does not fit in host memory. */
+SIGMO_API int sigmo_candidates_digest(sigmo_candidates_t c, uint64_t* digest);
+
+/* ---- signatures (signature::Signature<PowerGraph,4>, signature.hpp:20-391) */
+typedef struct sigmo_signature_s* sigmo_signature_t;
+
+/* Signature(queue, data_nodes, query_nodes): zeroed signatures and reachables
+ * (signature.hpp:157-168; the reference leaves reachables unzeroed). */
+SIGMO_API int sigmo_signature_create(sigmo_queue_t q, uint64_t data_nodes, uint64_t query_nodes, sigmo_signature_t* out);
+SIGMO_API int sigmo_signature_destroy(sigmo_signature_t s);
+/* generate{Data,Query}Signatures -> generateCSRSignatures (signature.hpp:57-69,125-152). */
+SIGMO_API int sigmo_signature_generate(sigmo_signature_t s, sigmo_graph_t g, int scope);
+/* refine{Data,Query}Signatures(g, view_size) -> refineCSRSignatures<PowerGraph>
+ * (signature.hpp:62-74,336-390). */
+SIGMO_API int sigmo_signature_refine(sigmo_signature_t s, sigmo_graph_t g, int scope, uint32_t view_size);
+/* Copy the current signatures of a scope to host (uint64 per vertex). */
+SIGMO_API int sigmo_signature_download(sigmo_signature_t s, int scope, uint64_t* host, uint64_t count);
+/* getData/QuerySignatureAllocationSize (signature.hpp:181-198). */
+SIGMO_API int sigmo_signature_alloc_size(sigmo_signature_t s, int scope, uint64_t* bytes);
+
+/* ---- filter / refine (isomorphism::filter, isomorphism.hpp:22-127) -------- */
+/* filterCandidates<Query> (isomorphism.hpp:22-62). */
+SIGMO_API int sigmo_filter_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_signature_t s,
+                            sigmo_candidates_t c);
+/* refineCandidates<Query> (isomorphism.hpp:64-127), race-free. */
+SIGMO_API int sigmo_refine_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_signature_t s,
+                            sigmo_candidates_t c);
+
+/* ---- GMCR mapping (isomorphism::mapping::GMCR, gmcr.hpp:16-131) ---------- */
+typedef struct sigmo_gmcr_s* sigmo_gmcr_t;
+
+SIGMO_API int sigmo_gmcr_create(sigmo_queue_t q, sigmo_gmcr_t* out);          /* GMCR(queue) gmcr.hpp:26 */
+SIGMO_API int sigmo_gmcr_destroy(sigmo_gmcr_t m);
+/* generateGMCR (gmcr.hpp:33-128).  Query ids within a data graph's segment
+ * are ascending; queries with <= 1 vertex are never admitted. */
+SIGMO_API int sigmo_gmcr_generate(sigmo_gmcr_t m, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c);
+/* total_query_indices (gmcr.hpp:81-82). */
+SIGMO_API int sigmo_gmcr_total(sigmo_gmcr_t m, uint64_t* total);
+/* data_graph_offsets [num_data_graphs+1] and query_graph_indices [total]. */
+SIGMO_API int sigmo_gmcr_download(sigmo_gmcr_t m, uint32_t* offsets, uint64_t offsets_len, uint32_t* indices,
+                        uint64_t indices_len);
+
+/* ---- join (isomorphism::join::joinCandidates, isomorphism.hpp:270-381) ---- */
+/* Adds the number of matches to *num_matches (host, caller-zeroed, like the
+ * reference's USM counter, sigmo.cpp:145-146).  find_first: at most one match
+ * per (query, data graph) pair.  per_pair (nullable, host) receives the count
+ * of every GMCR slot (total_query_indices entries). */
+SIGMO_API int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c,
+                          sigmo_gmcr_t m, uint64_t* num_matches, int find_first, uint64_t* per_pair);
+
+/* ---- batched form: whole pipeline in one call ----------------------------
+ * Signatures for iterations 1..R, fused label filter + R refinements (final
+ * bitset written once), GMCR and the persistent work-stealing join — the same
+ * results as the stage-per-launch calls above (sigmo.cpp:98-160), without host
+ * synchronisation between stages.  The GMCR and per-pair counts stay on the
+ * device in `m` / the result; totals are returned to the host. */
+typedef struct sigmo_match_result {
+  uint64_t total_matches;     /* sum over admitted pairs                     */
+  uint64_t admitted_pairs;    /* total_query_indices of the GMCR             */
+  uint64_t pairs;             /* num_query_graphs x num_data_graphs           */
+  double ms_signatures;       /* device time per stage (CUDA events)         */
+  double ms_filter;
+  double ms_mapping;
+  double ms_join;
+  double ms_total;
+} sigmo_match_result;
+
+SIGMO_API int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t iterations,
+                        int find_first, sigmo_candidates_t c, sigmo_gmcr_t m, sigmo_match_result* out);
+/* Per-pair counts of the last sigmo_match_batched call on `m` (GMCR slot order). */
+SIGMO_API int sigmo_match_download_counts(sigmo_gmcr_t m, uint64_t* per_pair, uint64_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIGMO_B200_H */

@@ -1,0 +1,480 @@
+"""sigmo_b200: B200-native (sm_100a) SIGMo hot path behind a C ABI.
+
+This Python layer mirrors the reference's C++ host API (namespace sigmo,
+library/include/*.hpp) over ctypes bindings of libsigmo_b200.so:
+
+  io.loadCSRGraphsFromFile / io.loadCSRGraphsFromLines      io.hpp:46-55
+  createDeviceCSRGraph / destroyDeviceCSRGraph              graph.hpp:255-322
+  candidates.Candidates                                      candidates.hpp:14-204
+  signature.Signature (PowerGraph, 4-bit counters)           signature.hpp:20-391
+  isomorphism.filter.filterCandidates / refineCandidates     isomorphism.hpp:22-127
+  isomorphism.mapping.GMCR                                   gmcr.hpp:16-131
+  isomorphism.join.joinCandidates                            isomorphism.hpp:270-381
+
+`sycl::queue` becomes `Queue` (a CUDA stream plus options).  Every call runs
+on the GPU; there is no CPU fallback: if the library is missing or no GPU is
+present the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+from types import SimpleNamespace
+
+import numpy as np
+
+from . import _lib as _L
+from ._lib import SigmoError, check, lib
+
+REF_PTX, REF_X86, EXACT = 0, 1, 2
+PROFILE_NAMES = {"ref-ptx": REF_PTX, "ref-x86": REF_X86, "exact": EXACT}
+SCOPE_DATA, SCOPE_QUERY = 0, 1
+
+__all__ = [
+    "SigmoError", "HostGraphs", "Queue", "DeviceBatchedCSRGraph", "createDeviceCSRGraph", "destroyDeviceCSRGraph",
+    "io", "candidates", "signature", "isomorphism", "generate_molecules", "generate_queries", "match_batched",
+    "REF_PTX", "EXACT",
+]
+
+
+def library_path() -> Path:
+    return _L.LIB_PATH
+
+
+# ---- host graphs ---------------------------------------------------------------
+class HostGraphs:
+    """A batch of graphs on the host in the batched CSR layout with global ids
+    (what createDeviceCSRGraph builds before copying, graph.hpp:255-294).
+    Owned by the library; the numpy views stay valid while this object lives."""
+
+    def __init__(self, raw: _L.HostGraphsC):
+        self._raw = raw
+
+    def __del__(self):
+        try:
+            lib().sigmo_host_graphs_free(ctypes.byref(self._raw))
+        except Exception:
+            pass
+
+    def _view(self, name, dtype, n):
+        ptr = getattr(self._raw, name)
+        if n == 0 or not ptr:
+            return np.zeros(0, dtype)
+        ct = {np.uint32: ctypes.c_uint32, np.uint8: ctypes.c_uint8}[dtype]
+        arr = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ct)), shape=(n,))
+        arr.flags.writeable = False
+        return arr
+
+    @property
+    def num_graphs(self) -> int:
+        return int(self._raw.num_graphs)
+
+    @property
+    def total_nodes(self) -> int:
+        return int(self._raw.total_nodes)
+
+    @property
+    def total_edges(self) -> int:
+        return int(self._raw.total_edges)
+
+    @property
+    def graph_offsets(self):
+        return self._view("graph_offsets", np.uint32, self.num_graphs + 1)
+
+    @property
+    def row_offsets(self):
+        return self._view("row_offsets", np.uint32, self.total_nodes + 1)
+
+    @property
+    def column_indices(self):
+        return self._view("column_indices", np.uint32, self.total_edges)
+
+    @property
+    def node_labels(self):
+        return self._view("node_labels", np.uint8, self.total_nodes)
+
+    @property
+    def edge_labels(self):
+        return self._view("edge_labels", np.uint8, self.total_edges)
+
+    def __len__(self):
+        return self.num_graphs
+
+    def sizes(self) -> np.ndarray:
+        return np.diff(self.graph_offsets.astype(np.int64))
+
+    def slice(self, first: int, count: int) -> "HostGraphs":
+        out = _L.HostGraphsC()
+        check(lib().sigmo_host_graphs_slice(ctypes.byref(self._raw), first, count, ctypes.byref(out)))
+        return HostGraphs(out)
+
+    def concat(self, other: "HostGraphs") -> "HostGraphs":
+        out = _L.HostGraphsC()
+        check(lib().sigmo_host_graphs_concat(ctypes.byref(self._raw), ctypes.byref(other._raw), ctypes.byref(out)))
+        return HostGraphs(out)
+
+    def to_text(self) -> str:
+        n = ctypes.c_size_t(0)
+        check(lib().sigmo_format_graphs(ctypes.byref(self._raw), None, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        check(lib().sigmo_format_graphs(ctypes.byref(self._raw), buf, ctypes.byref(n)))
+        return buf.raw[: n.value].decode()
+
+    @staticmethod
+    def from_text(text: str) -> "HostGraphs":
+        data = text.encode()
+        out = _L.HostGraphsC()
+        check(lib().sigmo_parse_graphs(data, len(data), ctypes.byref(out)))
+        return HostGraphs(out)
+
+
+def _load_lines(lines) -> HostGraphs:
+    return HostGraphs.from_text("\n".join(lines))
+
+
+def _load_file(path) -> HostGraphs:
+    return HostGraphs.from_text(Path(path).read_text())
+
+
+io = SimpleNamespace(loadCSRGraphsFromFile=_load_file, loadCSRGraphsFromLines=_load_lines, parse=HostGraphs.from_text)
+
+
+def generate_molecules(count: int, min_atoms: int = 10, max_atoms: int = 40, seed: int = 1, kind: int = 0,
+                       median: float = 22.0) -> HostGraphs:
+    out = _L.HostGraphsC()
+    check(lib().sigmo_generate_molecules(kind, count, min_atoms, max_atoms, median, seed, ctypes.byref(out)))
+    return HostGraphs(out)
+
+
+def generate_queries(count: int, min_atoms: int = 4, max_atoms: int = 12, seed: int = 2, kind: int = 0,
+                     skew_lo: int = 0, skew_hi: int = 0) -> HostGraphs:
+    out = _L.HostGraphsC()
+    check(lib().sigmo_generate_queries(kind, count, min_atoms, max_atoms, skew_lo, skew_hi, seed, ctypes.byref(out)))
+    return HostGraphs(out)
+
+
+# ---- queue --------------------------------------------------------------------------
+class BatchedEvent:
+    """utils::BatchedEvent (utils.hpp:127-161): device time of a stage."""
+
+    def __init__(self, queue: "Queue"):
+        self._ms = None
+        self._queue = queue
+        v = ctypes.c_double(0)
+        check(lib().sigmo_queue_last_stage_ms(queue._h, ctypes.byref(v)))
+        self._ms = v.value
+
+    def wait(self):
+        self._queue.wait()
+
+    def getProfilingInfo(self) -> float:
+        """Seconds of device time (the reference returns duration<double>)."""
+        return self._ms / 1e3
+
+
+class Queue:
+    """sycl::queue replacement: a CUDA stream on one device plus the options
+    of device::DeviceOptions (device.hpp:17-21) and the semantics profile."""
+
+    def __init__(self, device: int = 0, profile="ref-ptx", join_work_group_size: int = 128,
+                 filter_work_group_size: int = 512):
+        if isinstance(profile, str):
+            profile = PROFILE_NAMES[profile]
+        opts = _L.OptionsC(int(profile), join_work_group_size, filter_work_group_size)
+        h = ctypes.c_void_p()
+        check(lib().sigmo_queue_create(device, ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+        self.profile = int(profile)
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sigmo_queue_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def wait(self):
+        check(lib().sigmo_queue_wait(self._h))
+
+    wait_and_throw = wait
+
+    @property
+    def stream(self) -> int:
+        p = ctypes.c_void_p()
+        check(lib().sigmo_queue_stream(self._h, ctypes.byref(p)))
+        return p.value or 0
+
+    def launch_count(self) -> int:
+        v = ctypes.c_uint64()
+        check(lib().sigmo_queue_launch_count(self._h, ctypes.byref(v)))
+        return v.value
+
+    def device_info(self):
+        mem = ctypes.c_uint64()
+        name = ctypes.create_string_buffer(256)
+        check(lib().sigmo_queue_device_info(self._h, ctypes.byref(mem), name, 256))
+        return mem.value, name.value.decode()
+
+
+# ---- device graphs -------------------------------------------------------------------
+class DeviceBatchedCSRGraph:
+    """DeviceBatchedCSRGraph (graph.hpp:62-112) held on the device."""
+
+    def __init__(self, queue: Queue, handle):
+        self._queue = queue
+        self._h = handle
+        ng, tn, te, mx = ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        check(lib().sigmo_graph_info(handle, ctypes.byref(ng), ctypes.byref(tn), ctypes.byref(te), ctypes.byref(mx)))
+        self.num_graphs, self.total_nodes, self.total_edges, self.max_graph_nodes = ng.value, tn.value, te.value, mx.value
+
+    def destroy(self):
+        if getattr(self, "_h", None):
+            lib().sigmo_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def alloc_size(self) -> int:
+        v = ctypes.c_uint64()
+        check(lib().sigmo_graph_alloc_size(self._h, ctypes.byref(v)))
+        return v.value
+
+
+def createDeviceCSRGraph(queue: Queue, graphs: HostGraphs) -> DeviceBatchedCSRGraph:
+    h = ctypes.c_void_p()
+    check(lib().sigmo_graph_create(queue._h, ctypes.byref(graphs._raw), ctypes.byref(h)))
+    return DeviceBatchedCSRGraph(queue, h)
+
+
+def createDeviceCSRGraphFromDevice(queue: Queue, num_graphs: int, total_nodes: int, total_edges: int, graph_offsets: int,
+                                   row_offsets: int, column_indices: int, node_labels: int,
+                                   edge_labels: int) -> DeviceBatchedCSRGraph:
+    """Wrap five device-resident arrays (raw device pointers) without copying."""
+    h = ctypes.c_void_p()
+    check(lib().sigmo_graph_create_device(queue._h, num_graphs, total_nodes, total_edges, graph_offsets, row_offsets,
+                                          column_indices, node_labels, edge_labels, ctypes.byref(h)))
+    return DeviceBatchedCSRGraph(queue, h)
+
+
+def destroyDeviceCSRGraph(graph: DeviceBatchedCSRGraph, queue: Queue | None = None):
+    graph.destroy()
+
+
+def getDeviceGraphAllocSize(graph: DeviceBatchedCSRGraph) -> int:
+    return graph.alloc_size()
+
+
+# ---- candidates ------------------------------------------------------------------------
+class Candidates:
+    """candidates::Candidates (candidates.hpp:14-204): query-vertex-major bit
+    matrix, zero-filled at construction."""
+
+    def __init__(self, queue: Queue, source_nodes: int, target_nodes: int):
+        h = ctypes.c_void_p()
+        check(lib().sigmo_candidates_create(queue._h, source_nodes, target_nodes, ctypes.byref(h)))
+        self._h, self._queue = h, queue
+        self.source_nodes, self.target_nodes = source_nodes, target_nodes
+        self.single_node_size = (target_nodes + 31) // 32
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sigmo_candidates_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def getHostCandidates(self, row0: int = 0, rows: int | None = None) -> np.ndarray:
+        """Dense [rows][single_node_size] uint32 copy (candidates.hpp:185-190)."""
+        if rows is None:
+            rows = self.source_nodes - row0
+        out = np.zeros((rows, self.single_node_size), np.uint32)
+        check(lib().sigmo_candidates_download(self._h, row0, rows, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def getCandidatesCounts(self) -> np.ndarray:
+        out = np.zeros(self.source_nodes, np.uint32)
+        check(lib().sigmo_candidates_row_counts(self._h, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def getCandidatesCount(self, source_node: int) -> int:
+        """getCandidatesCount(source) (candidates.hpp:77-81)."""
+        return int(np.unpackbits(self.getHostCandidates(source_node, 1).view(np.uint8)).sum())
+
+    def getAllocationSize(self) -> int:
+        v = ctypes.c_uint64()
+        check(lib().sigmo_candidates_alloc_size(self._h, ctypes.byref(v)))
+        return v.value
+
+    def digest(self) -> int:
+        v = ctypes.c_uint64()
+        check(lib().sigmo_candidates_digest(self._h, ctypes.byref(v)))
+        return v.value
+
+
+# ---- signatures --------------------------------------------------------------------------
+class Signature:
+    """signature::Signature<PowerGraph, 4> (signature.hpp:20-391)."""
+
+    def __init__(self, queue: Queue, data_nodes: int, query_nodes: int):
+        h = ctypes.c_void_p()
+        check(lib().sigmo_signature_create(queue._h, data_nodes, query_nodes, ctypes.byref(h)))
+        self._h, self._queue = h, queue
+        self.data_nodes, self.query_nodes = data_nodes, query_nodes
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sigmo_signature_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _gen(self, g, scope):
+        check(lib().sigmo_signature_generate(self._h, g._h, scope))
+        return BatchedEvent(self._queue)
+
+    def _ref(self, g, scope, view):
+        check(lib().sigmo_signature_refine(self._h, g._h, scope, view))
+        return BatchedEvent(self._queue)
+
+    def generateDataSignatures(self, g):
+        return self._gen(g, SCOPE_DATA)
+
+    def generateQuerySignatures(self, g):
+        return self._gen(g, SCOPE_QUERY)
+
+    def refineDataSignatures(self, g, view_size: int = 1):
+        return self._ref(g, SCOPE_DATA, view_size)
+
+    def refineQuerySignatures(self, g, view_size: int = 1):
+        return self._ref(g, SCOPE_QUERY, view_size)
+
+    def _download(self, scope, n):
+        out = np.zeros(n, np.uint64)
+        check(lib().sigmo_signature_download(self._h, scope, out.ctypes.data_as(ctypes.c_void_p), n))
+        return out
+
+    def getDataSignatures(self) -> np.ndarray:
+        return self._download(SCOPE_DATA, self.data_nodes)
+
+    def getQuerySignatures(self) -> np.ndarray:
+        return self._download(SCOPE_QUERY, self.query_nodes)
+
+    @staticmethod
+    def getMaxLabels() -> int:
+        return 16
+
+
+# ---- filter / mapping / join ----------------------------------------------------------------
+def filterCandidates(queue: Queue, query_graph, data_graph, signatures: Signature, candidates: Candidates):
+    check(lib().sigmo_filter_candidates(queue._h, query_graph._h, data_graph._h, signatures._h, candidates._h))
+    return BatchedEvent(queue)
+
+
+def refineCandidates(queue: Queue, query_graph, data_graph, signatures: Signature, candidates: Candidates):
+    check(lib().sigmo_refine_candidates(queue._h, query_graph._h, data_graph._h, signatures._h, candidates._h))
+    return BatchedEvent(queue)
+
+
+class GMCR:
+    """isomorphism::mapping::GMCR (gmcr.hpp:16-131)."""
+
+    def __init__(self, queue: Queue):
+        h = ctypes.c_void_p()
+        check(lib().sigmo_gmcr_create(queue._h, ctypes.byref(h)))
+        self._h, self._queue = h, queue
+        self._num_data_graphs = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sigmo_gmcr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def generateGMCR(self, query_graphs, data_graphs, candidates: Candidates):
+        check(lib().sigmo_gmcr_generate(self._h, query_graphs._h, data_graphs._h, candidates._h))
+        self._num_data_graphs = data_graphs.num_graphs
+        return BatchedEvent(self._queue)
+
+    @property
+    def total_query_indices(self) -> int:
+        v = ctypes.c_uint64()
+        check(lib().sigmo_gmcr_total(self._h, ctypes.byref(v)))
+        return v.value
+
+    def getGMCR(self):
+        """(data_graph_offsets, query_graph_indices) on the host."""
+        off = np.zeros(self._num_data_graphs + 1, np.uint32)
+        tot = self.total_query_indices
+        idx = np.zeros(max(tot, 1), np.uint32)
+        check(lib().sigmo_gmcr_download(self._h, off.ctypes.data_as(ctypes.c_void_p), len(off),
+                                        idx.ctypes.data_as(ctypes.c_void_p), len(idx)))
+        return off, idx[:tot]
+
+    def getPairCounts(self) -> np.ndarray:
+        """Per-slot match counts of the last join / batched match on this GMCR."""
+        tot = self.total_query_indices
+        out = np.zeros(max(tot, 1), np.uint64)
+        check(lib().sigmo_match_download_counts(self._h, out.ctypes.data_as(ctypes.c_void_p), len(out)))
+        return out[:tot]
+
+
+def joinCandidates(queue: Queue, query_graphs, data_graphs, candidates: Candidates, gmcr: GMCR, num_matches,
+                   find_first: bool = True, per_pair: bool = False):
+    """isomorphism::join::joinCandidates (isomorphism.hpp:270-381).
+    num_matches: a one-element numpy uint64 array (the reference's USM
+    counter), incremented by the number of matches."""
+    acc = ctypes.c_uint64(int(num_matches[0]))
+    pp = None
+    if per_pair:
+        pp = np.zeros(max(gmcr.total_query_indices, 1), np.uint64)
+    check(lib().sigmo_join_candidates(queue._h, query_graphs._h, data_graphs._h, candidates._h, gmcr._h,
+                                      ctypes.byref(acc), int(bool(find_first)),
+                                      pp.ctypes.data_as(ctypes.c_void_p) if pp is not None else None))
+    num_matches[0] = acc.value
+    ev = BatchedEvent(queue)
+    if per_pair:
+        return ev, pp[: gmcr.total_query_indices]
+    return ev
+
+
+def match_batched(queue: Queue, query_graphs, data_graphs, iterations: int, find_first: bool,
+                  candidates: Candidates, gmcr: GMCR) -> dict:
+    """The batched form: signatures for all iterations, fused filter, GMCR and
+    the persistent join in one call (same results as the stage calls)."""
+    res = _L.MatchResultC()
+    check(lib().sigmo_match_batched(queue._h, query_graphs._h, data_graphs._h, iterations, int(bool(find_first)),
+                                    candidates._h, gmcr._h, ctypes.byref(res)))
+    gmcr._num_data_graphs = data_graphs.num_graphs
+    return {f: getattr(res, f) for f, _ in _L.MatchResultC._fields_}
+
+
+candidates = SimpleNamespace(Candidates=Candidates)
+signature = SimpleNamespace(Signature=Signature)
+isomorphism = SimpleNamespace(
+    filter=SimpleNamespace(filterCandidates=filterCandidates, refineCandidates=refineCandidates),
+    mapping=SimpleNamespace(GMCR=GMCR),
+    join=SimpleNamespace(joinCandidates=joinCandidates),
+)

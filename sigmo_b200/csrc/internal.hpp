@@ -1,0 +1,147 @@
+// Handle types and launch plumbing of the sigmo_b200 CUDA library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "common.hpp"
+#include "device.cuh"
+
+namespace sigmo_b200 {
+
+#define SIGMO_CUDA_TRY(expr)                                                                       \
+  do {                                                                                             \
+    cudaError_t _e = (expr);                                                                       \
+    if (_e != cudaSuccess)                                                                         \
+      return ::sigmo_b200::fail(_e == cudaErrorMemoryAllocation ? SIGMO_ERR_OOM : SIGMO_ERR_CUDA, \
+                                "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, \
+                                __LINE__);                                                         \
+  } while (0)
+
+#define SIGMO_TRY(expr)      \
+  do {                       \
+    int _rc = (expr);        \
+    if (_rc != SIGMO_OK) return _rc; \
+  } while (0)
+
+struct Queue {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  sigmo_options opts{};
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+  bool stage_recorded = false;
+  uint64_t launches = 0;
+  // Scratch reused by stages (grown on demand, freed with the queue).
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  void* pinned = nullptr;  // small pinned host buffer for scalar read-backs
+};
+
+struct Graph {
+  Queue* q = nullptr;
+  bool owned = true;
+  uint32_t num_graphs = 0;
+  uint64_t total_nodes = 0, total_edges = 0;
+  uint32_t* graph_offsets = nullptr;
+  uint32_t* row_offsets = nullptr;
+  uint32_t* column_indices = nullptr;
+  uint8_t* node_labels = nullptr;
+  uint8_t* edge_labels = nullptr;
+  // Derived on the device at creation:
+  uint32_t max_nodes = 0;          // largest graph
+  uint32_t adj_words = 1;          // u64 words per local adjacency row (<= 4)
+  uint32_t* node_graph = nullptr;  // [total_nodes] graph id of each vertex
+  uint64_t* adj = nullptr;         // [total_nodes * adj_words] local neighbour sets
+  uint8_t* sym = nullptr;          // [num_graphs] 1 if the adjacency is mirrored
+  uint32_t low_offset_graphs = 0;  // graphs whose first vertex is < 256
+  // Query-side matching orders (built on first use by the batched join):
+  uint8_t* qorder = nullptr;       // [total_nodes] local id placed at level k
+  uint64_t* qsel = nullptr;        // [total_nodes] adjacency to earlier levels
+  uint64_t* qsel_id = nullptr;     // [total_nodes] same, identity order
+  std::vector<uint32_t> host_graph_offsets;  // host copy (sizes, dispatch)
+};
+
+struct Candidates {
+  Queue* q = nullptr;
+  uint64_t rows = 0;     // source_nodes (query vertices)
+  uint64_t targets = 0;  // target_nodes (data vertices)
+  uint64_t W = 0;        // reference words per row: ceil(targets / 32)
+  uint64_t Wp = 0;       // device row stride in words (W rounded up to 32)
+  uint32_t* bits = nullptr;
+  bool known_zero = true;  // no bit set since the last zero fill
+};
+
+struct Signature {
+  Queue* q = nullptr;
+  uint64_t data_nodes = 0, query_nodes = 0;
+  uint64_t* data_sig = nullptr;
+  uint64_t* query_sig = nullptr;
+  uint64_t* data_reach = nullptr;
+  uint64_t* query_reach = nullptr;
+  uint32_t reach_words = 1;  // 1 (REF_PTX) or 4 (EXACT)
+  uint32_t* data_planes = nullptr;  // bit-sliced data signatures [16][Wp] x uint4
+  uint64_t planes_Wp = 0;
+  bool planes_valid = false;
+};
+
+struct Gmcr {
+  Queue* q = nullptr;
+  uint32_t num_data_graphs = 0;
+  uint32_t* offsets = nullptr;  // [num_data_graphs + 1]
+  uint32_t* indices = nullptr;  // [capacity]
+  uint32_t* pair_graph = nullptr;  // data graph of each slot [capacity]
+  uint64_t* counts = nullptr;   // per-slot match counts of the last join
+  uint64_t total = 0;
+  uint64_t capacity = 0;
+  bool counts_valid = false;
+};
+
+// Stage timing: every public stage brackets its launches with these.
+int stage_begin(Queue* q);
+int stage_end(Queue* q);
+
+// Stream-ordered device allocation on the queue's stream.
+int dev_alloc(Queue* q, void** p, size_t bytes);
+void dev_free(Queue* q, void* p);
+// Queue-owned scratch of at least `bytes` (contents undefined).
+int queue_scratch(Queue* q, size_t bytes, void** p);
+
+inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap = 0x7FFFFFFFu) {
+  uint64_t g = (work + block - 1) / block;
+  if (g == 0) g = 1;
+  return static_cast<unsigned>(g < cap ? g : cap);
+}
+
+int check_launch(Queue* q, const char* what);
+
+// ---- kernel launchers (defined in the .cu files) --------------------------
+int launch_graph_derive(Graph* g);
+int launch_query_order(Graph* g);
+int launch_sig_generate(Queue* q, const Graph* g, uint64_t* sig);
+int launch_sig_refine(Queue* q, const Graph* g, uint32_t view, uint64_t* sig, uint64_t* reach, uint32_t reach_words);
+int launch_sig_all(Queue* q, const Graph* g, uint32_t R, uint64_t* sig_all /* [R][N] */);
+int launch_sig_planes(Queue* q, const uint64_t* sig, uint64_t n, uint64_t Wp, uint32_t* planes);
+int launch_filter(Queue* q, const Graph* query, const Graph* data, Candidates* c);
+int launch_refine(Queue* q, const Graph* query, const Graph* data, const uint64_t* qsig, const uint32_t* planes,
+                  Candidates* c);
+int launch_fused_filter(Queue* q, const Graph* query, const Graph* data, uint32_t R, const uint64_t* qsig_all,
+                        const uint32_t* planes_all, Candidates* c);
+int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, bool sync_total,
+                uint64_t capacity_hint);
+int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
+                        uint32_t graph_begin, uint32_t graph_end, uint64_t* d_total);
+int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
+                     uint64_t* d_total);
+int launch_row_counts(Queue* q, const Candidates* c, uint32_t* d_counts);
+int launch_digest(Queue* q, const Candidates* c, uint64_t* d_digest);
+
+}  // namespace sigmo_b200
+
+// The opaque handle types of the C ABI are the internal structs.
+struct sigmo_queue_s : sigmo_b200::Queue {};
+struct sigmo_graph_s : sigmo_b200::Graph {};
+struct sigmo_candidates_s : sigmo_b200::Candidates {};
+struct sigmo_signature_s : sigmo_b200::Signature {};
+struct sigmo_gmcr_s : sigmo_b200::Gmcr {};

@@ -1,0 +1,186 @@
+// GMCR: the query-graph -> data-graph mapping (isomorphism::mapping::GMCR,
+// library/include/gmcr.hpp:33-128).  A pair (query graph q, data graph g) is
+// admitted when every vertex of q has at least one range-masked candidate in
+// g (getCandidatesCount(q_i, start_g, end_g) > 0, candidates.hpp:86-104).
+//
+// Instead of evaluating the predicate per pair twice with a serial scan in
+// between, the mapping is built from one streaming pass over the bitset:
+//   1. NE[j][g/32]: bit g = query vertex j has a candidate in data graph g
+//      (one read of the bitset; lane = data graph, ballot per 32 graphs);
+//   2. admit[q][g/32] = AND of NE over q's vertices, and per-graph counts;
+//   3. a device scan of the counts (the segment offsets);
+//   4. the fill, writing each segment's query ids in ascending order.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
+
+#include "internal.hpp"
+
+namespace sigmo_b200 {
+namespace {
+
+constexpr unsigned kNeRowsPerBlock = 32;
+
+__device__ __forceinline__ bool range_nonempty(const uint32_t* __restrict__ row, uint32_t s, uint32_t e, int prof) {
+  const uint32_t i0 = s >> 5, i1 = (e + 31u) >> 5;
+  for (uint32_t i = i0; i < i1; ++i)
+    if (row[i] & range_mask(i, s, e, prof)) return true;
+  return false;
+}
+
+__global__ void k_gmcr_ne(const uint32_t* __restrict__ bits, uint64_t Wp, uint64_t Qn, const uint32_t* __restrict__ dgoff,
+                          uint32_t G, uint32_t GW, int prof, uint32_t* __restrict__ NE) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (gw >= GW) return;
+  const uint32_t g = gw * 32u + lane;
+  uint32_t s = 0, e = 0;
+  if (g < G) {
+    s = dgoff[g];
+    e = dgoff[g + 1];
+  }
+  const uint64_t j0 = static_cast<uint64_t>(blockIdx.y) * kNeRowsPerBlock;
+  const uint64_t j1 = j0 + kNeRowsPerBlock < Qn ? j0 + kNeRowsPerBlock : Qn;
+  for (uint64_t j = j0; j < j1; ++j) {
+    const bool ne = g < G && range_nonempty(bits + j * Wp, s, e, prof);
+    const uint32_t word = __ballot_sync(0xFFFFFFFFu, ne);
+    if (lane == 0) NE[j * GW + gw] = word;
+  }
+}
+
+// Warp per 32 data graphs; lanes take query graphs 32 at a time.
+__global__ void k_gmcr_admit(const uint32_t* __restrict__ NE, uint32_t GW, const uint32_t* __restrict__ qgoff, uint32_t QG,
+                             uint32_t G, uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t gw = warp; gw < GW; gw += nwarps) {
+    const uint32_t valid = (G - gw * 32u) >= 32u ? 0xFFFFFFFFu : ((1u << (G - gw * 32u)) - 1u);
+    uint32_t cnt = 0;
+    for (uint32_t q0 = 0; q0 < QG; q0 += 32) {
+      const uint32_t q = q0 + lane;
+      uint32_t a = 0;
+      if (q < QG) {
+        const uint32_t off = qgoff[q], n = qgoff[q + 1] - off;
+        if (n > 1) {
+          a = valid;
+          for (uint32_t j = 0; j < n && a; ++j) a &= NE[static_cast<uint64_t>(off + j) * GW + gw];
+        }
+        admit[static_cast<uint64_t>(q) * GW + gw] = a;
+      }
+#pragma unroll 8
+      for (unsigned b = 0; b < 32; ++b) {
+        const uint32_t c = __popc(__ballot_sync(0xFFFFFFFFu, (a >> b) & 1u));
+        if (lane == b) cnt += c;
+      }
+    }
+    const uint32_t g = gw * 32u + lane;
+    if (g < G) counts[g] = cnt;
+  }
+}
+
+// Segment fill: lane = data graph; query ids visited in ascending order, so
+// every segment is sorted.
+__global__ void k_gmcr_fill(const uint32_t* __restrict__ admit, uint32_t GW, uint32_t QG, uint32_t G,
+                            const uint32_t* __restrict__ offsets, uint32_t* __restrict__ indices,
+                            uint32_t* __restrict__ pair_graph, uint64_t capacity) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t gw = warp; gw < GW; gw += nwarps) {
+    const uint32_t g = gw * 32u + lane;
+    uint64_t cur = g < G ? offsets[g] : 0;
+    for (uint32_t q = 0; q < QG; ++q) {
+      const uint32_t a = admit[static_cast<uint64_t>(q) * GW + gw];
+      if (!a) continue;
+      if ((a >> lane) & 1u) {
+        if (cur < capacity) {
+          indices[cur] = q;
+          pair_graph[cur] = g;
+        }
+        ++cur;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+// Builds m->offsets / indices / pair_graph.  With sync_total the total is read
+// back and the index arrays sized exactly (the reference reads it back too,
+// gmcr.hpp:80); otherwise capacity_hint bounds them.
+int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, bool sync_total,
+                uint64_t capacity_hint) {
+  const uint32_t G = data->num_graphs, QG = query->num_graphs;
+  const uint32_t GW = (G + 31u) / 32u;
+  const uint64_t Qn = query->total_nodes;
+  if (m->offsets && m->num_data_graphs != G) {
+    dev_free(q, m->offsets);
+    m->offsets = nullptr;
+  }
+  if (!m->offsets) SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&m->offsets), sizeof(uint32_t) * (G + 1ull)));
+  m->num_data_graphs = G;
+  m->counts_valid = false;
+  SIGMO_CUDA_TRY(cudaMemsetAsync(m->offsets, 0, sizeof(uint32_t) * (G + 1ull), q->stream));
+
+  // scratch: NE [Qn][GW], admit [QG][GW], counts [G], cub temp
+  const uint64_t ne_words = Qn * GW, admit_words = static_cast<uint64_t>(QG) * GW;
+  size_t cub_bytes = 0;
+  if (G) cub::DeviceScan::InclusiveSum(nullptr, cub_bytes, static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                       static_cast<int>(G), q->stream);
+  auto al = [](size_t x) { return (x + 255) & ~static_cast<size_t>(255); };
+  const size_t bytes = al(ne_words * 4) + al(admit_words * 4) + al(G * 4ull) + al(cub_bytes) + 256;
+  void* scratch = nullptr;
+  SIGMO_TRY(queue_scratch(q, bytes, &scratch));
+  char* p = static_cast<char*>(scratch);
+  uint32_t* NE = reinterpret_cast<uint32_t*>(p);
+  p += al(ne_words * 4);
+  uint32_t* admit = reinterpret_cast<uint32_t*>(p);
+  p += al(admit_words * 4);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(p);
+  p += al(G * 4ull);
+  void* cub_tmp = p;
+
+  if (G && QG && Qn) {
+    dim3 grid_ne((GW + 7u) / 8u, static_cast<unsigned>((Qn + kNeRowsPerBlock - 1) / kNeRowsPerBlock));
+    if (grid_ne.y > 65535u) return fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", (unsigned long long)Qn);
+    k_gmcr_ne<<<grid_ne, 256, 0, q->stream>>>(c->bits, c->Wp, Qn, data->graph_offsets, G, GW, q->opts.profile, NE);
+    SIGMO_TRY(check_launch(q, "k_gmcr_ne"));
+    k_gmcr_admit<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(NE, GW, query->graph_offsets, QG, G, admit, counts);
+    SIGMO_TRY(check_launch(q, "k_gmcr_admit"));
+    SIGMO_CUDA_TRY(cub::DeviceScan::InclusiveSum(cub_tmp, cub_bytes, counts, m->offsets + 1, static_cast<int>(G), q->stream));
+    q->launches++;
+  }
+
+  uint64_t cap;
+  if (sync_total) {
+    uint32_t* pinned = static_cast<uint32_t*>(q->pinned);
+    SIGMO_CUDA_TRY(cudaMemcpyAsync(pinned, m->offsets + G, sizeof(uint32_t), cudaMemcpyDeviceToHost, q->stream));
+    SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));
+    m->total = *pinned;
+    cap = m->total;
+  } else {
+    cap = capacity_hint;
+  }
+  if (cap > m->capacity || !m->indices) {
+    dev_free(q, m->indices);
+    dev_free(q, m->pair_graph);
+    dev_free(q, m->counts);
+    m->indices = m->pair_graph = nullptr;
+    m->counts = nullptr;
+    m->capacity = 0;
+    const uint64_t n = cap ? cap : 1;
+    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&m->indices), sizeof(uint32_t) * n));
+    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&m->pair_graph), sizeof(uint32_t) * n));
+    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&m->counts), sizeof(uint64_t) * n));
+    m->capacity = cap;
+  }
+  if (G && QG && Qn) {
+    k_gmcr_fill<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(admit, GW, QG, G, m->offsets, m->indices,
+                                                                                m->pair_graph, m->capacity);
+    SIGMO_TRY(check_launch(q, "k_gmcr_fill"));
+  }
+  return SIGMO_OK;
+}
+
+}  // namespace sigmo_b200

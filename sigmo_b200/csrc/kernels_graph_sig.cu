@@ -1,0 +1,413 @@
+// Graph-derived device structures and the signature kernels.
+//
+// Signatures follow Signature<PowerGraph,4> (library/include/signature.hpp):
+// generateCSRSignatures (:125-152) and refineCSRSignatures<PowerGraph>
+// (:336-390).  The refinement is a bounded BFS per vertex; here each graph's
+// local adjacency is kept as one bit row per vertex (u64 words, local ids), so
+// a BFS level is an OR of rows selected by the frontier's bits.
+#include <cuda_runtime.h>
+
+#include "internal.hpp"
+
+namespace sigmo_b200 {
+namespace {
+
+__global__ void k_node_graph(const uint32_t* __restrict__ goff, uint32_t G, uint32_t* __restrict__ node_graph) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+    const uint32_t v1 = goff[g + 1];
+    for (uint32_t v = goff[g]; v < v1; ++v) node_graph[v] = g;
+  }
+}
+
+// Local adjacency rows: bit t of row v = (prev + t) appears in v's CSR row,
+// for local ids t < 64 * AW (prev = first vertex of v's graph).
+template <int AW>
+__global__ void k_build_adj(uint64_t N, const uint32_t* __restrict__ roff, const uint32_t* __restrict__ col,
+                            const uint32_t* __restrict__ goff, const uint32_t* __restrict__ node_graph,
+                            uint64_t* __restrict__ adj) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < N; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t prev = goff[node_graph[v]];
+    uint64_t row[AW];
+#pragma unroll
+    for (int k = 0; k < AW; ++k) row[k] = 0;
+    for (uint32_t i = roff[v]; i < roff[v + 1]; ++i) {
+      const uint32_t t = col[i] - prev;
+      if (t < 64u * AW) {
+#pragma unroll
+        for (int k = 0; k < AW; ++k)
+          if ((t >> 6) == (uint32_t)k) row[k] |= 1ull << (t & 63u);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < AW; ++k) adj[v * AW + k] = row[k];
+  }
+}
+
+// generateCSRSignatures (signature.hpp:136-146): +1 per neighbour label, on
+// top of the current value.
+__global__ void k_sig_generate(uint64_t N, const uint32_t* __restrict__ roff, const uint32_t* __restrict__ col,
+                               const uint8_t* __restrict__ lab, uint64_t* __restrict__ sig) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < N; v += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t s = sig[v];
+    for (uint32_t i = roff[v]; i < roff[v + 1]; ++i) s = sig_inc(s, lab[col[i]]);
+    sig[v] = s;
+  }
+}
+
+// REF_PTX BFS for graphs of more than 256 vertices: the reference's bitset
+// truncates local ids to uint8_t, so vertex t occupies bit (t & 255) when that
+// is < 64 and no bit otherwise; bit b is expanded through vertex prev + b.
+__device__ uint64_t ptx_wide_ball(uint32_t v, uint32_t prev, uint32_t view, const uint32_t* __restrict__ roff,
+                                  const uint32_t* __restrict__ col, uint64_t* self_bit) {
+  const uint64_t self = refbit(v - prev, 0);
+  uint64_t F = self, R = self;
+  for (uint32_t it = 0; it < view && F; ++it) {
+    uint64_t nx = 0, m = F;
+    while (m) {
+      const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
+      m &= m - 1;
+      const uint32_t u = prev + b;
+      for (uint32_t i = roff[u]; i < roff[u + 1]; ++i) nx |= refbit(col[i] - prev, 0);
+    }
+    nx &= ~R;
+    R |= nx;
+    F = nx;
+  }
+  *self_bit = self;
+  return R;
+}
+
+// refineCSRSignatures<PowerGraph> (signature.hpp:348-386), REF_PTX profile:
+// sphere = ball_view(v) \ {v} \ old(v); sig = label histogram of the sphere;
+// old |= sphere.  Local ids >= 64 have no bit (graph sizes <= 256).
+__global__ void k_sig_refine_ptx(uint64_t N, const uint32_t* __restrict__ goff, const uint32_t* __restrict__ node_graph,
+                                 const uint64_t* __restrict__ adj, uint32_t AW, const uint32_t* __restrict__ roff,
+                                 const uint32_t* __restrict__ col, const uint8_t* __restrict__ lab, uint32_t view,
+                                 uint64_t* __restrict__ sig, uint64_t* __restrict__ reach) {
+  for (uint64_t vv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; vv < N; vv += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = static_cast<uint32_t>(vv);
+    const uint32_t g = node_graph[v];
+    const uint32_t prev = goff[g], n = goff[g + 1] - prev;
+    uint64_t self, R;
+    if (n > 256u) {
+      R = ptx_wide_ball(v, prev, view, roff, col, &self);
+    } else {
+      const uint32_t lv = v - prev;
+      self = lv < 64u ? (1ull << lv) : 0ull;
+      uint64_t F = self;
+      R = self;
+      for (uint32_t it = 0; it < view && F; ++it) {
+        uint64_t nx = 0, m = F;
+        while (m) {
+          const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
+          m &= m - 1;
+          nx |= adj[static_cast<uint64_t>(prev + b) * AW];
+        }
+        nx &= ~R;
+        R |= nx;
+        F = nx;
+      }
+    }
+    R &= ~self;
+    const uint64_t old = reach[v];
+    uint64_t sphere = R & ~old;
+    const uint64_t keep = sphere;
+    uint64_t s = 0;
+    while (sphere) {
+      const uint32_t b = __ffsll(static_cast<long long>(sphere)) - 1;
+      sphere &= sphere - 1;
+      s = sig_inc(s, lab[prev + b]);
+    }
+    sig[v] = s;
+    reach[v] = keep | old;
+  }
+}
+
+// EXACT profile: true local sets of up to 64*AW vertices.
+template <int AW>
+__global__ void k_sig_refine_exact(uint64_t N, const uint32_t* __restrict__ goff, const uint32_t* __restrict__ node_graph,
+                                   const uint64_t* __restrict__ adj, const uint8_t* __restrict__ lab, uint32_t view,
+                                   uint64_t* __restrict__ sig, uint64_t* __restrict__ reach) {
+  for (uint64_t vv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; vv < N; vv += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = static_cast<uint32_t>(vv);
+    const uint32_t prev = goff[node_graph[v]];
+    const uint32_t lv = v - prev;
+    uint64_t F[AW], R[AW];
+#pragma unroll
+    for (int k = 0; k < AW; ++k) F[k] = R[k] = ((lv >> 6) == (uint32_t)k) ? (1ull << (lv & 63u)) : 0ull;
+    for (uint32_t it = 0; it < view; ++it) {
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < AW; ++k) any |= F[k] != 0;
+      if (!any) break;
+      uint64_t nx[AW];
+#pragma unroll
+      for (int k = 0; k < AW; ++k) nx[k] = 0;
+#pragma unroll
+      for (int w = 0; w < AW; ++w) {
+        uint64_t m = F[w];
+        while (m) {
+          const uint32_t b = __ffsll(static_cast<long long>(m)) - 1 + 64u * w;
+          m &= m - 1;
+          const uint64_t* row = adj + static_cast<uint64_t>(prev + b) * AW;
+#pragma unroll
+          for (int k = 0; k < AW; ++k) nx[k] |= row[k];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < AW; ++k) {
+        nx[k] &= ~R[k];
+        R[k] |= nx[k];
+        F[k] = nx[k];
+      }
+    }
+    uint64_t s = 0;
+#pragma unroll
+    for (int k = 0; k < AW; ++k) {
+      if ((lv >> 6) == (uint32_t)k) R[k] &= ~(1ull << (lv & 63u));
+      uint64_t* old = reach + static_cast<uint64_t>(v) * kMaxAdjWords + k;
+      uint64_t sphere = R[k] & ~*old;
+      *old |= R[k];
+      while (sphere) {
+        const uint32_t b = __ffsll(static_cast<long long>(sphere)) - 1;
+        sphere &= sphere - 1;
+        s = sig_inc(s, lab[prev + 64u * k + b]);
+      }
+    }
+    sig[v] = s;
+  }
+}
+
+// All refinement iterations 1..R at once (batched form): starting from empty
+// reachables, iteration r's sphere is exactly BFS level r, so one BFS to
+// depth R emits every iteration's signature.  sig_all is [R][N].
+template <int AW, bool EXACT>
+__global__ void k_sig_all(uint64_t N, const uint32_t* __restrict__ goff, const uint32_t* __restrict__ node_graph,
+                          const uint64_t* __restrict__ adj, const uint32_t* __restrict__ roff,
+                          const uint32_t* __restrict__ col, const uint8_t* __restrict__ lab, uint32_t Rn,
+                          uint64_t* __restrict__ sig_all) {
+  for (uint64_t vv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; vv < N; vv += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = static_cast<uint32_t>(vv);
+    const uint32_t prev = goff[node_graph[v]];
+    const uint32_t n = goff[node_graph[v] + 1] - prev;
+    const uint32_t lv = v - prev;
+    uint64_t F[AW], R[AW];
+    const bool wide = !EXACT && n > 256u;
+#pragma unroll
+    for (int k = 0; k < AW; ++k) F[k] = 0;
+    if (EXACT) {
+#pragma unroll
+      for (int k = 0; k < AW; ++k) F[k] = ((lv >> 6) == (uint32_t)k) ? (1ull << (lv & 63u)) : 0ull;
+    } else {
+      F[0] = wide ? refbit(lv, 0) : (lv < 64u ? (1ull << lv) : 0ull);
+    }
+#pragma unroll
+    for (int k = 0; k < AW; ++k) R[k] = F[k];
+    for (uint32_t r = 0; r < Rn; ++r) {
+      uint64_t nx[AW];
+#pragma unroll
+      for (int k = 0; k < AW; ++k) nx[k] = 0;
+      if (EXACT) {
+#pragma unroll
+        for (int w = 0; w < AW; ++w) {
+          uint64_t m = F[w];
+          while (m) {
+            const uint32_t b = __ffsll(static_cast<long long>(m)) - 1 + 64u * w;
+            m &= m - 1;
+            const uint64_t* row = adj + static_cast<uint64_t>(prev + b) * AW;
+#pragma unroll
+            for (int k = 0; k < AW; ++k) nx[k] |= row[k];
+          }
+        }
+      } else {
+        uint64_t m = F[0];
+        while (m) {
+          const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
+          m &= m - 1;
+          if (wide) {
+            const uint32_t u = prev + b;
+            for (uint32_t i = roff[u]; i < roff[u + 1]; ++i) nx[0] |= refbit(col[i] - prev, 0);
+          } else {
+            nx[0] |= adj[static_cast<uint64_t>(prev + b) * AW];
+          }
+        }
+      }
+      uint64_t s = 0;
+#pragma unroll
+      for (int k = 0; k < AW; ++k) {
+        nx[k] &= ~R[k];
+        R[k] |= nx[k];
+        F[k] = nx[k];
+        uint64_t sphere = nx[k];
+        while (sphere) {
+          const uint32_t b = __ffsll(static_cast<long long>(sphere)) - 1;
+          sphere &= sphere - 1;
+          s = sig_inc(s, lab[prev + 64u * k + b]);
+        }
+        if (!EXACT) break;
+      }
+      sig_all[static_cast<uint64_t>(r) * N + v] = s;
+    }
+  }
+}
+
+// Matching order per query graph (batched join): start at the vertex of
+// highest degree, then repeatedly take the vertex with the most neighbours
+// already placed (ties: higher degree, lower id).  qorder[off + k] = local id
+// placed at level k; qsel[off + k] = levels i < k adjacent to level k in that
+// order; qsel_id[off + k] = the same for the identity order (used when a graph
+// has an asymmetric adjacency, which only self-loops produce).  sym[g] = 1 if
+// every adjacency row of graph g is mirrored.
+__global__ void k_query_order(uint32_t QG, const uint32_t* __restrict__ goff, const uint64_t* __restrict__ adj,
+                              uint8_t* __restrict__ qorder, uint64_t* __restrict__ qsel, uint64_t* __restrict__ qsel_id) {
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < QG; q += gridDim.x * blockDim.x) {
+    const uint32_t off = goff[q], n = goff[q + 1] - off;
+    if (n > kMaxQueryNodes) continue;
+    uint64_t placed = 0;
+    uint8_t ord[kMaxQueryNodes];
+    for (uint32_t k = 0; k < n; ++k) {
+      int best = -1, best_conn = -1, best_deg = -1;
+      for (uint32_t u = 0; u < n; ++u) {
+        if ((placed >> u) & 1ull) continue;
+        const uint64_t row = adj[off + u];
+        const int conn = __popcll(row & placed);
+        const int deg = __popcll(row);
+        if (conn > best_conn || (conn == best_conn && deg > best_deg)) {
+          best = static_cast<int>(u);
+          best_conn = conn;
+          best_deg = deg;
+        }
+      }
+      ord[k] = static_cast<uint8_t>(best);
+      placed |= 1ull << best;
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+      uint64_t sel = 0, sel_id = 0;
+      for (uint32_t i = 0; i < k; ++i) {
+        if ((adj[off + ord[i]] >> ord[k]) & 1ull) sel |= 1ull << i;
+        if ((adj[off + i] >> k) & 1ull) sel_id |= 1ull << i;
+      }
+      qorder[off + k] = ord[k];
+      qsel[off + k] = sel;
+      qsel_id[off + k] = sel_id;
+    }
+  }
+}
+
+template <int AW>
+__global__ void k_graph_symmetric(uint32_t G, const uint32_t* __restrict__ goff, const uint64_t* __restrict__ adj,
+                                  uint8_t* __restrict__ sym) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+    const uint32_t off = goff[g], n = goff[g + 1] - off;
+    bool ok = n <= 64u * AW;
+    for (uint32_t u = 0; u < n && ok; ++u)
+      for (uint32_t t = 0; t < n && ok; ++t) {
+        const bool a = (adj[static_cast<uint64_t>(off + u) * AW + (t >> 6)] >> (t & 63u)) & 1ull;
+        const bool b = (adj[static_cast<uint64_t>(off + t) * AW + (u >> 6)] >> (u & 63u)) & 1ull;
+        ok = a == b;
+      }
+    sym[g] = ok ? 1 : 0;
+  }
+}
+
+}  // namespace
+
+int launch_graph_derive(Graph* g) {
+  Queue* q = g->q;
+  const unsigned B = 256;
+  if (g->total_nodes) {
+    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&g->node_graph), sizeof(uint32_t) * g->total_nodes));
+    k_node_graph<<<grid_for(g->num_graphs, B, 65535u), B, 0, q->stream>>>(g->graph_offsets, g->num_graphs, g->node_graph);
+    SIGMO_TRY(check_launch(q, "k_node_graph"));
+  }
+  uint32_t mx = g->max_nodes;
+  uint32_t aw = (mx + 63u) / 64u;
+  if (aw < 1) aw = 1;
+  if (aw > kMaxAdjWords) aw = kMaxAdjWords;
+  g->adj_words = aw;
+  const uint64_t adj_elems = g->total_nodes * aw;
+  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&g->adj), sizeof(uint64_t) * (adj_elems ? adj_elems : 1)));
+  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&g->sym), g->num_graphs ? g->num_graphs : 1));
+  if (g->total_nodes) {
+    const unsigned grid = grid_for(g->total_nodes, B, 148u * 32u);
+    switch (aw) {
+      case 1: k_build_adj<1><<<grid, B, 0, q->stream>>>(g->total_nodes, g->row_offsets, g->column_indices, g->graph_offsets, g->node_graph, g->adj); break;
+      case 2: k_build_adj<2><<<grid, B, 0, q->stream>>>(g->total_nodes, g->row_offsets, g->column_indices, g->graph_offsets, g->node_graph, g->adj); break;
+      default: k_build_adj<4><<<grid, B, 0, q->stream>>>(g->total_nodes, g->row_offsets, g->column_indices, g->graph_offsets, g->node_graph, g->adj); break;
+    }
+    SIGMO_TRY(check_launch(q, "k_build_adj"));
+  }
+  if (g->num_graphs) {
+    const unsigned grid = grid_for(g->num_graphs, B, 148u * 32u);
+    switch (aw) {
+      case 1: k_graph_symmetric<1><<<grid, B, 0, q->stream>>>(g->num_graphs, g->graph_offsets, g->adj, g->sym); break;
+      case 2: k_graph_symmetric<2><<<grid, B, 0, q->stream>>>(g->num_graphs, g->graph_offsets, g->adj, g->sym); break;
+      default: k_graph_symmetric<4><<<grid, B, 0, q->stream>>>(g->num_graphs, g->graph_offsets, g->adj, g->sym); break;
+    }
+    SIGMO_TRY(check_launch(q, "k_graph_symmetric"));
+  }
+  return SIGMO_OK;
+}
+
+int launch_query_order(Graph* g) {
+  Queue* q = g->q;
+  if (g->qorder) return SIGMO_OK;
+  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&g->qorder), g->total_nodes ? g->total_nodes : 1));
+  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&g->qsel), sizeof(uint64_t) * (g->total_nodes ? g->total_nodes : 1)));
+  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&g->qsel_id), sizeof(uint64_t) * (g->total_nodes ? g->total_nodes : 1)));
+  if (g->num_graphs && g->adj_words == 1) {
+    k_query_order<<<grid_for(g->num_graphs, 128, 4096u), 128, 0, q->stream>>>(g->num_graphs, g->graph_offsets, g->adj,
+                                                                               g->qorder, g->qsel, g->qsel_id);
+    SIGMO_TRY(check_launch(q, "k_query_order"));
+  }
+  return SIGMO_OK;
+}
+
+int launch_sig_generate(Queue* q, const Graph* g, uint64_t* sig) {
+  if (!g->total_nodes) return SIGMO_OK;
+  k_sig_generate<<<grid_for(g->total_nodes, 256, 148u * 32u), 256, 0, q->stream>>>(g->total_nodes, g->row_offsets,
+                                                                                   g->column_indices, g->node_labels, sig);
+  return check_launch(q, "k_sig_generate");
+}
+
+int launch_sig_refine(Queue* q, const Graph* g, uint32_t view, uint64_t* sig, uint64_t* reach, uint32_t reach_words) {
+  if (!g->total_nodes) return SIGMO_OK;
+  const unsigned grid = grid_for(g->total_nodes, 256, 148u * 32u);
+  if (q->opts.profile == kProfileExact) {
+    if (g->max_nodes > 64u * kMaxAdjWords)
+      return fail(SIGMO_ERR_DOMAIN, "exact profile supports graphs of at most %u vertices (largest: %u)", 64u * kMaxAdjWords, g->max_nodes);
+    if (reach_words != kMaxAdjWords) return fail(SIGMO_ERR_INVALID, "exact profile needs %u reachable words", kMaxAdjWords);
+    switch (g->adj_words) {
+      case 1: k_sig_refine_exact<1><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->node_labels, view, sig, reach); break;
+      case 2: k_sig_refine_exact<2><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->node_labels, view, sig, reach); break;
+      default: k_sig_refine_exact<4><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->node_labels, view, sig, reach); break;
+    }
+    return check_launch(q, "k_sig_refine_exact");
+  }
+  k_sig_refine_ptx<<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->adj_words,
+                                                g->row_offsets, g->column_indices, g->node_labels, view, sig, reach);
+  return check_launch(q, "k_sig_refine_ptx");
+}
+
+int launch_sig_all(Queue* q, const Graph* g, uint32_t R, uint64_t* sig_all) {
+  if (!g->total_nodes || !R) return SIGMO_OK;
+  const unsigned grid = grid_for(g->total_nodes, 256, 148u * 32u);
+  if (q->opts.profile == kProfileExact) {
+    if (g->max_nodes > 64u * kMaxAdjWords)
+      return fail(SIGMO_ERR_DOMAIN, "exact profile supports graphs of at most %u vertices (largest: %u)", 64u * kMaxAdjWords, g->max_nodes);
+    switch (g->adj_words) {
+      case 1: k_sig_all<1, true><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+      case 2: k_sig_all<2, true><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+      default: k_sig_all<4, true><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+    }
+    return check_launch(q, "k_sig_all<exact>");
+  }
+  switch (g->adj_words) {
+    case 1: k_sig_all<1, false><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+    case 2: k_sig_all<2, false><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+    default: k_sig_all<4, false><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+  }
+  return check_launch(q, "k_sig_all<ptx>");
+}
+
+}  // namespace sigmo_b200
