@@ -1,0 +1,475 @@
+#!/usr/bin/env python
+"""Benchmark of the SIGMo hot path on B200: query x molecule pairs/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sigmo|reference]
+
+A step is one pass of the whole hot path (signatures for iterations 1..R,
+label filter + R refinements, GMCR mapping, join with per-pair uint64 counts)
+over one batch.  The default workload is 100,000 seeded synthetic molecules
+(10-60 heavy atoms) x 600 queries (3-30 atoms, 70% in 6-15), 6 refinement
+iterations, find-all, REF_PTX semantics.
+
+value: pairs/s of the batched form with the graphs resident in HBM (device
+time from CUDA events on the library's stream, max over ranks).  e2e: the same
+metric through the C ABI from pinned host buffers (graph upload + match +
+per-pair count read-back every step).  plain_form: the stage-per-launch form
+(reference driver order, host sync after every stage).  cpu_baseline: the
+CPU oracle (the reference's algorithm restated; the SYCL reference cannot be
+built here) on a bounded sample, all host threads.
+
+--impl reference times that CPU implementation alone (rank 0; other ranks
+exit 0) and prints the same JSON line with "impl": "reference".
+
+Multi-GPU (torchrun): data graphs are independent, so every rank runs its own
+replica of the workload (weak scaling, no data-path collective); the timing
+is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "query×molecule pairs/s (bit-exact) on 1 B200 vs plain form; p50/p99 batch latency"
+
+WORKLOADS = {
+    "drug100k": dict(
+        desc="100,000 synthetic molecules (10-60 atoms) x 600 queries (3-30 atoms, skewed 6-15), 6 refinement iterations",
+        mols=100_000, min_atoms=10, max_atoms=60, kind=0, median=22.0, queries=600, qmin=3, qmax=30, skew=(6, 15),
+        qkind=0, R=6, seed_d=20251, seed_q=20252),
+    "drug1k": dict(
+        desc="1,000 synthetic molecules (10-40 atoms) x 20 queries (4-12 atoms), 6 refinement iterations",
+        mols=1_000, min_atoms=10, max_atoms=40, kind=0, median=22.0, queries=20, qmin=4, qmax=12, skew=(0, 0),
+        qkind=0, R=6, seed_d=1001, seed_q=1002),
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["sigmo", "reference"], default="sigmo")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="drug100k")
+    ap.add_argument("--mode", choices=["find-all", "find-first"], default="find-all")
+    ap.add_argument("--profile", choices=["ref-ptx", "exact"], default="ref-ptx")
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-sample", type=int, default=10_000, help="molecules in the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---- distributed plumbing ----------------------------------------------------------
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def init_dist(world, backend):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(dist, value: float, device=None) -> float:
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- workload ----------------------------------------------------------------------
+def make_workload(wl, rank=0):
+    import sigmo_b200 as sb
+
+    d = sb.generate_molecules(wl["mols"], wl["min_atoms"], wl["max_atoms"], seed=wl["seed_d"] + 7919 * rank, kind=wl["kind"],
+                              median=wl["median"])
+    q = sb.generate_queries(wl["queries"], wl["qmin"], wl["qmax"], seed=wl["seed_q"], kind=wl["qkind"],
+                            skew_lo=wl["skew"][0], skew_hi=wl["skew"][1])
+    return q, d
+
+
+def cpu_baseline(q, d, wl, sample_mols, find_first, profile):
+    """The oracle (CPU restatement of the reference) on the first
+    `sample_mols` molecules x all queries, every host thread."""
+    import oracle
+
+    ds = d.slice(0, min(sample_mols, d.num_graphs))
+    prof = {"ref-ptx": oracle.REF_PTX, "exact": oracle.EXACT}[profile]
+    t0 = time.perf_counter()
+    out = oracle.run_pipeline(q, ds, wl["R"], prof, find_first)
+    dt = time.perf_counter() - t0
+    pairs = q.num_graphs * ds.num_graphs
+    return {
+        "value": pairs / dt,
+        "unit": "pairs/s",
+        "cores": int(oracle.lib().orc_num_threads()),
+        "kind": "port",
+        "sample": f"first {ds.num_graphs} molecules x {q.num_graphs} queries of the workload, full pipeline "
+                  f"({'find-first' if find_first else 'find-all'}, {wl['R']} iterations), {dt:.2f} s",
+        "matches": int(out["total"]),
+        "seconds": dt,
+    }
+
+
+# ---- clocks --------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- roofline -----------------------------------------------------------------------
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        j = json.loads(p.read_text())
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_for(kernel: str, workload: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    j = json.loads(p.read_text())
+    e = j.get(f"{kernel}@{workload}")
+    return None if e is None else e.get("bytes_per_launch")
+
+
+def fused_filter_bytes(Qn, N, R):
+    """Algorithmic HBM bytes of one fused filter launch: the final bitset
+    written once (4 B per 32 (query vertex, data vertex) pairs, rows padded
+    to 128 B), data labels read once, bit-sliced data signatures read once
+    (16 labels x 4 planes x 4 B per 32 data vertices per iteration) and the
+    query signatures / labels read once."""
+    W = (N + 31) // 32
+    Wp = (W + 31) // 32 * 32
+    return 4 * Qn * Wp + N + R * 16 * 16 * Wp + 8 * R * Qn + Qn
+
+
+# ---- the sigmo arm -------------------------------------------------------------------
+def run_sigmo(args, rank, world, local):
+    import torch
+
+    import sigmo_b200 as sb
+
+    wl = WORKLOADS[args.workload]
+    torch.cuda.set_device(local)
+    dist = init_dist(world, "nccl")
+    ff = args.mode == "find-first"
+    q, d = make_workload(wl, rank)
+    R = wl["R"]
+    pairs = q.num_graphs * d.num_graphs
+
+    queue = sb.Queue(local, profile=args.profile)
+    qg, dg = sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)
+    cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes)
+    gm = sb.GMCR(queue)
+    stream = torch.cuda.ExternalStream(queue.stream, device=local)
+
+    for _ in range(max(args.warmup, 0)):
+        res = sb.match_batched(queue, qg, dg, R, ff, cand, gm)
+    queue.wait()
+
+    # ---- timed region: K steps, device-resident inputs ----
+    step_ms, stage = [], []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = queue.launch_count()
+    with ClockSampler(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            res = sb.match_batched(queue, qg, dg, R, ff, cand, gm)
+            step_ms.append(res["ms_total"])
+            stage.append(res)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    launches = queue.launch_count() - launches0
+    elapsed_ms = ev0.elapsed_time(ev1)
+    elapsed_ms = max_over_ranks(dist, elapsed_ms, device=f"cuda:{local}")
+    ms_per_step = elapsed_ms / args.steps
+    value = world * pairs / (ms_per_step / 1e3)
+    total_matches = res["total_matches"]
+    admitted = res["admitted_pairs"]
+
+    # ---- per-stage device times (last steps) and the fused filter roofline ----
+    med = lambda k: statistics.median(s[k] for s in stage)  # noqa: E731
+    filt_ms = med("ms_filter")
+    hbm, peak_kind = peaks()
+    fb = fused_filter_bytes(qg.total_nodes, dg.total_nodes, R)
+    achieved = fb / (filt_ms / 1e3) / 1e9
+    tr = traffic_for("k_fused_filter", args.workload)
+    roof = {"kernel": "k_fused_filter", "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "traffic": tr, "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": fb, "ms_per_launch": round(filt_ms, 4)}
+    stages = {k: round(med(k), 4) for k in ("ms_signatures", "ms_filter", "ms_mapping", "ms_join", "ms_total")}
+
+    # ---- the plain stage-per-launch form (same results, reference order) ----
+    plain = None
+    if args.plain_steps > 0:
+        def plain_step():
+            sig = sb.Signature(queue, dg.total_nodes, qg.total_nodes)
+            c2 = sb.Candidates(queue, qg.total_nodes, dg.total_nodes)
+            sig.generateDataSignatures(dg)
+            sig.generateQuerySignatures(qg)
+            sb.filterCandidates(queue, qg, dg, sig, c2)
+            queue.wait()
+            for r in range(1, R + 1):
+                sig.refineDataSignatures(dg, r)
+                queue.wait()
+                sig.refineQuerySignatures(qg, r)
+                queue.wait()
+                sb.refineCandidates(queue, qg, dg, sig, c2)
+                queue.wait()
+            g2 = sb.GMCR(queue)
+            g2.generateGMCR(qg, dg, c2)
+            nm = np.zeros(1, np.uint64)
+            sb.joinCandidates(queue, qg, dg, c2, g2, nm, ff)
+            queue.wait()
+            dig = c2.digest()
+            adm = g2.total_query_indices
+            sig.close()
+            c2.close()
+            g2.close()
+            return int(nm[0]), dig, adm
+
+        plain_step()  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.plain_steps):
+            p_total, p_digest, p_adm = plain_step()
+        torch.cuda.synchronize()
+        p_ms = (time.perf_counter() - t0) * 1e3 / args.plain_steps
+        b_digest = cand.digest()
+        plain = {"value": pairs / (p_ms / 1e3), "unit": "pairs/s", "ms_per_step": round(p_ms, 3),
+                 "batched_over_plain": round((pairs / (ms_per_step / 1e3)) / (pairs / (p_ms / 1e3)), 3),
+                 "identical_results": bool(p_total == total_matches and p_digest == b_digest and p_adm == admitted)}
+
+    # ---- e2e through the C ABI from pinned host buffers ----
+    e2e = None
+    if args.e2e_steps > 0:
+        import ctypes
+
+        from sigmo_b200 import _lib as L
+
+        def pinned_copy(h):
+            arrs = {}
+            for f, dt in (("graph_offsets", torch.int32), ("row_offsets", torch.int32), ("column_indices", torch.int32),
+                          ("node_labels", torch.uint8), ("edge_labels", torch.uint8)):
+                a = np.asarray(getattr(h, f))
+                t = torch.empty(max(a.size, 1), dtype=dt, pin_memory=True)
+                t.numpy()[: a.size] = a.view(np.int32) if dt == torch.int32 else a
+                arrs[f] = t
+            raw = L.HostGraphsC(h.num_graphs, h.total_nodes, h.total_edges, arrs["graph_offsets"].data_ptr(),
+                                arrs["row_offsets"].data_ptr(), arrs["column_indices"].data_ptr(),
+                                arrs["node_labels"].data_ptr(), arrs["edge_labels"].data_ptr())
+            nbytes = sum(int(np.asarray(getattr(h, f)).nbytes) for f in arrs)
+            return raw, arrs, nbytes
+
+        qraw, qkeep, qbytes = pinned_copy(q)
+        draw, dkeep, dbytes = pinned_copy(d)
+        counts_host = torch.empty(max(admitted, 1), dtype=torch.int64, pin_memory=True)
+        lib = L.lib()
+
+        def e2e_step():
+            hq, hd = ctypes.c_void_p(), ctypes.c_void_p()
+            L.check(lib.sigmo_graph_create(queue._h, ctypes.byref(qraw), ctypes.byref(hq)))
+            L.check(lib.sigmo_graph_create(queue._h, ctypes.byref(draw), ctypes.byref(hd)))
+            r = L.MatchResultC()
+            L.check(lib.sigmo_match_batched(queue._h, hq, hd, R, int(ff), cand._h, gm._h, ctypes.byref(r)))
+            L.check(lib.sigmo_match_download_counts(gm._h, ctypes.c_void_p(counts_host.data_ptr()), counts_host.numel()))
+            lib.sigmo_graph_destroy(hq)
+            lib.sigmo_graph_destroy(hd)
+            return r.total_matches, r.admitted_pairs
+
+        e2e_step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            et, ea = e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        e_ms = max_over_ranks(dist, e0.elapsed_time(e1), device=f"cuda:{local}") / args.e2e_steps
+        e2e = {"value": world * pairs / (e_ms / 1e3), "unit": "pairs/s", "ms_per_step": round(e_ms, 3),
+               "h2d_bytes_per_step": qbytes + dbytes, "d2h_bytes_per_step": 8 * ea + 8,
+               "identical_results": bool(et == total_matches and ea == admitted)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(q, d, wl, args.cpu_sample, ff, args.profile)
+
+    if dist:
+        torch.cuda.synchronize()
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC,
+        "value": round(value, 1),
+        "unit": "pairs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded generator; SIGMo's SMARTS/ZINC sets are not available)",
+        "config": {"workload": args.workload + ": " + wl["desc"], "molecules": d.num_graphs, "queries": q.num_graphs,
+                   "data_vertices": d.total_nodes, "query_vertices": q.total_nodes, "iterations": R, "mode": args.mode,
+                   "profile": args.profile, "pairs_per_step_per_gpu": pairs,
+                   "l2": "inputs larger than L2: every step rewrites the %.2f GB candidate bitset" % (
+                       4 * cand.source_nodes * ((cand.single_node_size + 31) // 32 * 32) / 1e9),
+                   "parallelism": f"replicas{world}" if world > 1 else "single"},
+        "latency_ms": {"p50": round(float(np.percentile(step_ms, 50)), 3), "p99": round(float(np.percentile(step_ms, 99)), 3)},
+        "stages_ms": stages,
+        "admitted_pairs": admitted,
+        "total_matches": total_matches,
+        "roofline": roof,
+        "plain_form": plain,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+    }
+    print(json.dumps(out))
+
+
+# ---- the reference arm ------------------------------------------------------------------
+def run_reference(args, rank, world, local):
+    if rank != 0:
+        return
+    import oracle
+
+    wl = WORKLOADS[args.workload]
+    ff = args.mode == "find-first"
+    q, d = make_workload(wl, 0)
+    prof = {"ref-ptx": oracle.REF_PTX, "exact": oracle.EXACT}[args.profile]
+    sample = min(args.cpu_sample // 5 if args.cpu_sample >= 5 else 1, d.num_graphs) or 1
+    ds = d.slice(0, sample)
+    pairs = q.num_graphs * ds.num_graphs
+    for _ in range(max(args.warmup, 0)):
+        oracle.run_pipeline(q, ds, wl["R"], prof, ff)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out = oracle.run_pipeline(q, ds, wl["R"], prof, ff)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times) / len(times)
+    v = pairs / dt
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(v, 1),
+        "unit": "pairs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(dt * 1e3, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": args.workload + ": " + wl["desc"], "mode": args.mode, "profile": args.profile,
+                   "step_sample": f"first {ds.num_graphs} molecules x {q.num_graphs} queries per step"},
+        "latency_ms": {"p50": round(float(np.percentile(times, 50)) * 1e3, 3),
+                       "p99": round(float(np.percentile(times, 99)) * 1e3, 3)},
+        "cpu_baseline": {"value": round(v, 1), "unit": "pairs/s", "cores": int(oracle.lib().orc_num_threads()),
+                         "kind": "port",
+                         "sample": f"first {ds.num_graphs} molecules x {q.num_graphs} queries, full pipeline; the SYCL "
+                                   f"reference cannot be compiled here (no SYCL compiler), so its CPU restatement runs"},
+        "e2e": {"value": round(v, 1), "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "total_matches_sample": int(out["total"]),
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world, local)
+    else:
+        run_sigmo(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -14,6 +14,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libsigmo_b200.so"
+CLI = HERE / "sigmo_cli"
 INCLUDE = HERE.parent / "include"
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -40,7 +41,7 @@ def sources() -> list[Path]:
 
 def _fingerprint() -> str:
     h = hashlib.sha256()
-    for p in sorted(CSRC.iterdir()) + sorted(INCLUDE.glob("*.h")):
+    for p in sorted(CSRC.iterdir()) + sorted(INCLUDE.rglob("*.h*")) + sorted((HERE / "cli").glob("*")):
         if p.is_file():
             h.update(p.name.encode())
             h.update(p.read_bytes())
@@ -79,8 +80,21 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
     if verbose:
         sys.stderr.write(res.stdout + res.stderr)
+    build_cli(hc)
     stamp.write_text(fp)
     return LIB
+
+
+def build_cli(host_compiler: str | None = None) -> Path:
+    """The command-line driver (same flags and report as the reference's
+    sigmo driver), linked against the in-tree library."""
+    cxx = host_compiler or _host_compiler() or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-o", str(CLI), str(HERE / "cli" / "sigmo_main.cpp"), f"-L{HERE}", "-lsigmo_b200",
+           "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("building the CLI failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
+    return CLI
 
 
 if __name__ == "__main__":

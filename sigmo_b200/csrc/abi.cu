@@ -189,7 +189,8 @@ int sigmo_graph_create(sigmo_queue_t q, const sigmo_host_graphs* h, sigmo_graph_
   if (!q || !h || !out) return fail(SIGMO_ERR_INVALID, "sigmo_graph_create: null argument");
   *out = nullptr;
   SIGMO_TRY(set_device(q));
-  if (h->num_graphs && (!h->graph_offsets || !h->row_offsets)) return fail(SIGMO_ERR_INVALID, "sigmo_graph_create: null arrays");
+  if (!h->graph_offsets || !h->row_offsets || (h->total_edges && !h->column_indices) || (h->total_nodes && !h->node_labels))
+    return fail(SIGMO_ERR_INVALID, "sigmo_graph_create: null arrays");
   if (h->graph_offsets[h->num_graphs] != h->total_nodes || h->row_offsets[h->total_nodes] != h->total_edges)
     return fail(SIGMO_ERR_INVALID, "sigmo_graph_create: offsets disagree with totals");
   sigmo_graph_t g = new (std::nothrow) sigmo_graph_s();

@@ -26,13 +26,14 @@ __global__ void k_build_adj(uint64_t N, const uint32_t* __restrict__ roff, const
                             const uint32_t* __restrict__ goff, const uint32_t* __restrict__ node_graph,
                             uint64_t* __restrict__ adj) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < N; v += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t prev = goff[node_graph[v]];
+    const uint32_t g = node_graph[v];
+    const uint32_t prev = goff[g], n = goff[g + 1] - prev;
     uint64_t row[AW];
 #pragma unroll
     for (int k = 0; k < AW; ++k) row[k] = 0;
     for (uint32_t i = roff[v]; i < roff[v + 1]; ++i) {
-      const uint32_t t = col[i] - prev;
-      if (t < 64u * AW) {
+      const uint32_t t = col[i] - prev;  // neighbours outside the graph set no bit
+      if (t < n && t < 64u * AW) {
 #pragma unroll
         for (int k = 0; k < AW; ++k)
           if ((t >> 6) == (uint32_t)k) row[k] |= 1ull << (t & 63u);

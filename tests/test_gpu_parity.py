@@ -1,0 +1,231 @@
+"""GPU parity: every stage of the sm_100a path, called through the C ABI,
+against the oracle and the committed golden vectors — bit-exact signatures and
+candidate bitsets after every refinement iteration, identical GMCR, identical
+per-(query, data graph) counts in find-all and flags in find-first."""
+import json
+
+import numpy as np
+import pytest
+
+import oracle
+import sigmo_b200 as sb
+
+pytestmark = pytest.mark.gpu
+
+DEVICE_PROFILES = (oracle.REF_PTX, oracle.EXACT)
+
+
+def run_plain(qh, dh, R, profile, find_first, wg=128, keep=False):
+    """The reference driver's stage order (library/src/sigmo.cpp:98-160)."""
+    queue = sb.Queue(0, profile=profile, join_work_group_size=wg)
+    qg, dg = sb.createDeviceCSRGraph(queue, qh), sb.createDeviceCSRGraph(queue, dh)
+    cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes)
+    sig = sb.Signature(queue, dg.total_nodes, qg.total_nodes)
+    sig.generateDataSignatures(dg)
+    sig.generateQuerySignatures(qg)
+    sb.filterCandidates(queue, qg, dg, sig, cand)
+    hist = {"sig_data": [], "sig_query": [], "bitsets": []}
+
+    def snap():
+        if keep:
+            hist["sig_data"].append(sig.getDataSignatures())
+            hist["sig_query"].append(sig.getQuerySignatures())
+            hist["bitsets"].append(cand.getHostCandidates())
+
+    snap()
+    for r in range(1, R + 1):
+        sig.refineDataSignatures(dg, r)
+        sig.refineQuerySignatures(qg, r)
+        sb.refineCandidates(queue, qg, dg, sig, cand)
+        snap()
+    gm = sb.GMCR(queue)
+    gm.generateGMCR(qg, dg, cand)
+    nm = np.zeros(1, np.uint64)
+    _, per = sb.joinCandidates(queue, qg, dg, cand, gm, nm, find_first, per_pair=True)
+    off, idx = gm.getGMCR()
+    hist.update(offsets=off, indices=idx, per_pair=per, total=int(nm[0]), digest=cand.digest(),
+                final=cand.getHostCandidates() if keep else None, launches=queue.launch_count())
+    return hist
+
+
+def run_batched(qh, dh, R, profile, find_first, wg=128, keep_bits=False):
+    queue = sb.Queue(0, profile=profile, join_work_group_size=wg)
+    qg, dg = sb.createDeviceCSRGraph(queue, qh), sb.createDeviceCSRGraph(queue, dh)
+    cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes)
+    gm = sb.GMCR(queue)
+    res = sb.match_batched(queue, qg, dg, R, find_first, cand, gm)
+    off, idx = gm.getGMCR()
+    return {"offsets": off, "indices": idx, "per_pair": gm.getPairCounts(), "total": res["total_matches"],
+            "digest": cand.digest(), "final": cand.getHostCandidates() if keep_bits else None, "res": res}
+
+
+@pytest.fixture(scope="module")
+def golden(golden_dir):
+    return json.loads((golden_dir / "golden.json").read_text())
+
+
+def _golden_runs(golden):
+    for case in golden["cases"]:
+        for run in case["runs"]:
+            if run["profile"] in DEVICE_PROFILES:
+                yield case, run
+
+
+def test_plain_stages_match_golden(golden):
+    n = 0
+    for case, run in _golden_runs(golden):
+        qh, dh = sb.io.parse(case["query_text"]), sb.io.parse(case["data_text"])
+        R, prof = run["iterations"], run["profile"]
+        ctx = f"{case['name']} profile={prof} R={R}"
+        out = run_plain(qh, dh, R, prof, False, keep=True)
+        for it in range(R + 1):
+            assert out["sig_data"][it].tolist() == run["sig_data"][it], f"{ctx} data signatures, iteration {it}"
+            assert out["sig_query"][it].tolist() == run["sig_query"][it], f"{ctx} query signatures, iteration {it}"
+            assert out["bitsets"][it].tolist() == run["bitsets"][it], f"{ctx} bitset, iteration {it}"
+        assert out["offsets"].tolist() == run["offsets"], ctx
+        assert out["indices"].tolist() == run["indices"], ctx
+        assert out["per_pair"].tolist() == run["per_pair_all"], ctx
+        assert out["total"] == run["total_all"], ctx
+        first = run_plain(qh, dh, R, prof, True)
+        assert first["per_pair"].tolist() == run["per_pair_first"], ctx
+        assert first["total"] == run["total_first"], ctx
+        n += 1
+    assert n >= 15
+
+
+def test_batched_form_matches_golden(golden):
+    for case, run in _golden_runs(golden):
+        qh, dh = sb.io.parse(case["query_text"]), sb.io.parse(case["data_text"])
+        R, prof = run["iterations"], run["profile"]
+        ctx = f"{case['name']} profile={prof} R={R}"
+        for ff, key in ((False, "all"), (True, "first")):
+            out = run_batched(qh, dh, R, prof, ff, keep_bits=True)
+            assert out["final"].tolist() == run["bitsets"][-1], ctx
+            assert out["offsets"].tolist() == run["offsets"], ctx
+            assert out["indices"].tolist() == run["indices"], ctx
+            assert out["per_pair"].tolist() == run[f"per_pair_{key}"], f"{ctx} {key}"
+            assert out["total"] == run[f"total_{key}"], f"{ctx} {key}"
+
+
+def _oracle(qh, dh, R, prof, ff, wg=128, keep=False):
+    return oracle.run_pipeline(qh, dh, R, prof, ff, wg=wg, keep=keep)
+
+
+def _check(out, ref, ctx):
+    assert out["offsets"].tolist() == ref["offsets"].tolist(), ctx
+    assert out["indices"].tolist() == ref["indices"].tolist(), ctx
+    assert np.array_equal(out["per_pair"], ref["per_pair"]), ctx
+    assert out["total"] == ref["total"], ctx
+    assert out["digest"] == oracle.digest(ref["bits"]), ctx
+
+
+@pytest.mark.parametrize("prof", DEVICE_PROFILES)
+def test_small_drug_like_config(prof):
+    """1,000 molecules of 10-40 atoms, 20 queries of 4-12 atoms, 6 refinement
+    iterations, find-all and find-first; every iteration's bitset compared."""
+    dh = sb.generate_molecules(1000, 10, 40, seed=1001)
+    qh = sb.generate_queries(20, 4, 12, seed=1002)
+    R = 6
+    ref = _oracle(qh, dh, R, prof, False, keep=True)
+    out = run_plain(qh, dh, R, prof, False, keep=True)
+    for it in range(R + 1):
+        assert np.array_equal(out["sig_data"][it], ref["sig_data"][it]), it
+        assert np.array_equal(out["sig_query"][it], ref["sig_query"][it]), it
+        assert np.array_equal(out["bitsets"][it], ref["bitsets"][it]), it
+    _check(out, ref, "plain find-all")
+    _check(run_batched(qh, dh, R, prof, False), ref, "batched find-all")
+    ref1 = _oracle(qh, dh, R, prof, True)
+    _check(run_plain(qh, dh, R, prof, True), ref1, "plain find-first")
+    _check(run_batched(qh, dh, R, prof, True), ref1, "batched find-first")
+    assert ref["total"] > 0 and len(ref["indices"]) > 0
+
+
+@pytest.mark.parametrize("wg", [32, 64, 256])
+def test_join_work_group_sizes(wg):
+    """The literal join's pair-to-item assignment follows the work-group size."""
+    dh = sb.generate_molecules(120, 8, 30, seed=77)
+    qh = sb.generate_queries(300, 3, 8, seed=78)
+    ref = _oracle(qh, dh, 2, oracle.REF_PTX, False, wg=wg)
+    _check(run_plain(qh, dh, 2, oracle.REF_PTX, False, wg=wg), ref, f"plain wg={wg}")
+    _check(run_batched(qh, dh, 2, oracle.REF_PTX, False, wg=wg), ref, f"batched wg={wg}")
+
+
+@pytest.mark.parametrize("prof", DEVICE_PROFILES)
+def test_heavy_tail_graphs_over_64_atoms(prof):
+    dh = sb.generate_molecules(400, 6, 120, seed=31, kind=1, median=30)
+    assert int(dh.sizes().max()) > 64
+    qh = sb.generate_queries(25, 3, 12, seed=32)
+    for R in (1, 4):
+        ref = _oracle(qh, dh, R, prof, False, keep=True)
+        out = run_plain(qh, dh, R, prof, False, keep=True)
+        for it in range(R + 1):
+            assert np.array_equal(out["bitsets"][it], ref["bitsets"][it]), (R, it)
+        _check(out, ref, f"plain R={R}")
+        _check(run_batched(qh, dh, R, prof, False), ref, f"batched R={R}")
+
+
+@pytest.mark.parametrize("prof", DEVICE_PROFILES)
+def test_symmetry_stress_small(prof):
+    dh = sb.generate_molecules(150, 12, 50, seed=41, kind=2)
+    qh = sb.generate_queries(12, 4, 10, seed=42, kind=3)
+    ref = _oracle(qh, dh, 3, prof, False)
+    _check(run_plain(qh, dh, 3, prof, False), ref, "plain")
+    _check(run_batched(qh, dh, 3, prof, False), ref, "batched")
+    assert ref["per_pair"].max() >= 12  # automorphic patterns give many embeddings
+
+
+def test_edge_inputs():
+    # a single data graph, queries of 2 vertices, a 1-vertex query, a data graph
+    # with no edges, wildcard query labels and labels >= 16
+    q = "n#2 l#2 0 8 1 8 e#1 0 1 1\nn#1 l#1 0 8 e#0\nn#3 l#2 0 255 1 8 2 20 e#2 0 1 1 1 2 1\n"
+    d = ("n#5 l#3 0 8 1 8 2 20 3 7 4 8 e#4 0 1 1 1 2 1 2 3 1 3 4 1\n"
+         "n#3 l#1 0 8 1 8 2 8 e#0\n"
+         "n#4 l#2 0 8 1 20 2 8 3 8 e#3 0 1 1 1 2 1 2 3 1\n")
+    qh, dh = sb.io.parse(q), sb.io.parse(d)
+    for prof in DEVICE_PROFILES:
+        for R in (0, 3):
+            for ff in (False, True):
+                ref = _oracle(qh, dh, R, prof, ff)
+                _check(run_plain(qh, dh, R, prof, ff), ref, f"plain {prof} {R} {ff}")
+                _check(run_batched(qh, dh, R, prof, ff), ref, f"batched {prof} {R} {ff}")
+
+
+def test_graph_ending_on_word_boundary_masks():
+    """REF_PTX drops the last word of a multi-word range whose end is
+    32-aligned (candidates.hpp:98); EXACT keeps it."""
+    lines = ["n#20 l#1 " + " ".join(f"{i} 8" for i in range(20)) + " e#19 " + " ".join(f"{i} {i+1} 1" for i in range(19)),
+             "n#44 l#1 " + " ".join(f"{i} 8" for i in range(44)) + " e#43 " + " ".join(f"{i} {i+1} 1" for i in range(43))]
+    dh = sb.io.parse("\n".join(lines) + "\n")
+    qh = sb.io.parse("n#3 l#1 0 8 1 8 2 8 e#2 0 1 1 1 2 1\n")
+    outs = {}
+    for prof in DEVICE_PROFILES:
+        ref = _oracle(qh, dh, 0, prof, False)
+        out = run_plain(qh, dh, 0, prof, False)
+        _check(out, ref, str(prof))
+        _check(run_batched(qh, dh, 0, prof, False), ref, str(prof))
+        outs[prof] = out
+    assert outs[oracle.REF_PTX]["total"] != outs[oracle.EXACT]["total"]
+
+
+def test_stage_events_and_launch_count():
+    dh = sb.generate_molecules(200, 10, 30, seed=5)
+    qh = sb.generate_queries(10, 4, 8, seed=6)
+    queue = sb.Queue(0)
+    qg, dg = sb.createDeviceCSRGraph(queue, qh), sb.createDeviceCSRGraph(queue, dh)
+    sig = sb.Signature(queue, dg.total_nodes, qg.total_nodes)
+    ev = sig.generateDataSignatures(dg)
+    assert ev.getProfilingInfo() >= 0.0
+    assert queue.launch_count() > 0
+    mem, name = queue.device_info()
+    assert mem > 0 and name
+
+
+def test_mid_size_slice_against_oracle():
+    """20,000 molecules x 120 queries (a slice of the 100k x 600 workload's
+    generator), 6 iterations, both modes: device == oracle."""
+    dh = sb.generate_molecules(20000, 10, 60, seed=2024)
+    qh = sb.generate_queries(120, 3, 30, seed=2025, skew_lo=6, skew_hi=15)
+    for ff in (False, True):
+        ref = _oracle(qh, dh, 6, oracle.REF_PTX, ff)
+        _check(run_batched(qh, dh, 6, oracle.REF_PTX, ff), ref, f"batched ff={ff}")
+        _check(run_plain(qh, dh, 6, oracle.REF_PTX, ff), ref, f"plain ff={ff}")
