@@ -213,11 +213,16 @@ SIGMO_API int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_
                           sigmo_gmcr_t m, uint64_t* num_matches, int find_first, uint64_t* per_pair);
 
 /* ---- batched form: whole pipeline in one call ----------------------------
- * Signatures for iterations 1..R, fused label filter + R refinements (final
- * bitset written once), GMCR and the persistent work-stealing join — the same
- * results as the stage-per-launch calls above (sigmo.cpp:98-160), without host
- * synchronisation between stages.  The GMCR and per-pair counts stay on the
- * device in `m` / the result; totals are returned to the host. */
+ * Signatures for iterations 1..R in one BFS, per-data-graph candidate planes
+ * (one u64 vertex mask per distinct query label and per distinct (iteration,
+ * label, count) threshold), GMCR from the AND-programs of identical-vertex
+ * classes, and the persistent work-stealing join — the same GMCR and counts
+ * as the stage-per-launch calls (sigmo.cpp:98-160) with one host
+ * synchronisation.  The final candidate bitset is not written unless
+ * SIGMO_MATCH_MATERIALIZE_BITSET is given (then `c` receives it); `c` may be
+ * NULL otherwise.  GMCR and per-pair counts stay on the device in `m`. */
+enum { SIGMO_MATCH_MATERIALIZE_BITSET = 1 };
+
 typedef struct sigmo_match_result {
   uint64_t total_matches;     /* sum over admitted pairs                     */
   uint64_t admitted_pairs;    /* total_query_indices of the GMCR             */
@@ -230,7 +235,7 @@ typedef struct sigmo_match_result {
 } sigmo_match_result;
 
 SIGMO_API int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t iterations,
-                        int find_first, sigmo_candidates_t c, sigmo_gmcr_t m, sigmo_match_result* out);
+                        int find_first, uint32_t flags, sigmo_candidates_t c, sigmo_gmcr_t m, sigmo_match_result* out);
 /* Per-pair counts of the last sigmo_match_batched call on `m` (GMCR slot order). */
 SIGMO_API int sigmo_match_download_counts(sigmo_gmcr_t m, uint64_t* per_pair, uint64_t len);
 

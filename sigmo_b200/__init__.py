@@ -460,13 +460,19 @@ def joinCandidates(queue: Queue, query_graphs, data_graphs, candidates: Candidat
     return ev
 
 
+MATCH_MATERIALIZE_BITSET = 1
+
+
 def match_batched(queue: Queue, query_graphs, data_graphs, iterations: int, find_first: bool,
-                  candidates: Candidates, gmcr: GMCR) -> dict:
-    """The batched form: signatures for all iterations, fused filter, GMCR and
-    the persistent join in one call (same results as the stage calls)."""
+                  candidates: Candidates | None, gmcr: GMCR, materialize: bool = False) -> dict:
+    """The batched form: signatures for all iterations, candidate planes,
+    GMCR and the persistent join in one call (same GMCR and counts as the
+    stage calls).  With materialize=True the final candidate bitset is also
+    written into `candidates`."""
     res = _L.MatchResultC()
-    check(lib().sigmo_match_batched(queue._h, query_graphs._h, data_graphs._h, iterations, int(bool(find_first)),
-                                    candidates._h, gmcr._h, ctypes.byref(res)))
+    flags = MATCH_MATERIALIZE_BITSET if materialize else 0
+    check(lib().sigmo_match_batched(queue._h, query_graphs._h, data_graphs._h, iterations, int(bool(find_first)), flags,
+                                    candidates._h if candidates is not None else None, gmcr._h, ctypes.byref(res)))
     gmcr._num_data_graphs = data_graphs.num_graphs
     return {f: getattr(res, f) for f, _ in _L.MatchResultC._fields_}
 

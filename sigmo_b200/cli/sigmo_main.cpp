@@ -205,7 +205,8 @@ int main(int argc, char** argv) try {
     sigmo::isomorphism::mapping::GMCR gmcr{queue};
     sigmo_match_result r;
     sigmo::check(sigmo_match_batched(queue.handle(), dq.handle, dd.handle, static_cast<uint32_t>(args.refinement_steps),
-                                     args.find_all ? 0 : 1, candidates.handle(), gmcr.handle(), &r));
+                                     args.find_all ? 0 : 1, SIGMO_MATCH_MATERIALIZE_BITSET, candidates.handle(),
+                                     gmcr.handle(), &r));
     std::cout << "[*] Batched pipeline: signatures " << std::lround(r.ms_signatures) << " ms, filter " << std::lround(r.ms_filter)
               << " ms, mapping " << std::lround(r.ms_mapping) << " ms, join " << std::lround(r.ms_join) << " ms\n";
     dsig.push_back(std::chrono::duration<double>(r.ms_signatures / 1e3));

@@ -117,6 +117,14 @@ int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out
   if (st == cudaSuccess) st = cudaEventCreate(&q->ev_start);
   if (st == cudaSuccess) st = cudaEventCreate(&q->ev_end);
   if (st == cudaSuccess) st = cudaMallocHost(&q->pinned, 4096);
+  if (st == cudaSuccess) {
+    // Keep freed stream-ordered allocations cached in the device's default pool
+    // (per-call scratch is then reused instead of being remapped every call).
+    cudaMemPool_t pool;
+    st = cudaDeviceGetDefaultMemPool(&pool, device);
+    uint64_t threshold = UINT64_MAX;
+    if (st == cudaSuccess) st = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
   if (st != cudaSuccess) {
     int rc = fail(SIGMO_ERR_CUDA, "queue creation failed: %s", cudaGetErrorString(st));
     sigmo_queue_destroy(q);
@@ -277,6 +285,7 @@ int sigmo_graph_destroy(sigmo_graph_t g) {
   dev_free(q, g->qorder);
   dev_free(q, g->qsel);
   dev_free(q, g->qsel_id);
+  release_plane_program(g);
   delete g;
   return SIGMO_OK;
 }
@@ -602,82 +611,6 @@ int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t da
     }
   }
   dev_free(q, d_total);
-  return rc;
-}
-
-// ---- batched form -----------------------------------------------------------
-int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t R, int find_first,
-                        sigmo_candidates_t c, sigmo_gmcr_t m, sigmo_match_result* out) {
-  if (!q || !query || !data || !c || !m || !out) return fail(SIGMO_ERR_INVALID, "null argument");
-  if (c->rows != query->total_nodes || c->targets != data->total_nodes)
-    return fail(SIGMO_ERR_INVALID, "candidate bitset does not match the graphs");
-  if (m->q != q || c->q != q) return fail(SIGMO_ERR_INVALID, "handles belong to another queue");
-  SIGMO_TRY(set_device(q));
-  std::memset(out, 0, sizeof(*out));
-  cudaEvent_t ev[5];
-  for (auto& e : ev) SIGMO_CUDA_TRY(cudaEventCreate(&e));
-  struct EvGuard {
-    cudaEvent_t* e;
-    ~EvGuard() {
-      for (int i = 0; i < 5; ++i) cudaEventDestroy(e[i]);
-    }
-  } guard{ev};
-  const uint64_t N = data->total_nodes, Qn = query->total_nodes;
-  // scratch: data sig_all [R][N], query sig_all [R][Qn], planes [R][16][Wp] uint4, total
-  void* buf = nullptr;
-  const uint64_t b_dsig = 8ull * R * N, b_qsig = 8ull * R * Qn, b_planes = 16ull * 16 * R * c->Wp;
-  auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-  SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_qsig) + al(b_planes) + 256));
-  char* p = static_cast<char*>(buf);
-  uint64_t* dsig = reinterpret_cast<uint64_t*>(p);
-  p += al(b_dsig);
-  uint64_t* qsig = reinterpret_cast<uint64_t*>(p);
-  p += al(b_qsig);
-  uint32_t* planes = reinterpret_cast<uint32_t*>(p);
-  p += al(b_planes);
-  uint64_t* d_total = reinterpret_cast<uint64_t*>(p);
-  int rc = SIGMO_OK;
-  auto step = [&](int r) {
-    if (!rc) rc = r;
-  };
-  step(cudaEventRecord(ev[0], q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "event record failed"));
-  step(launch_sig_all(q, data, R, dsig));
-  step(launch_sig_all(q, query, R, qsig));
-  for (uint32_t r = 0; r < R && !rc; ++r)
-    step(launch_sig_planes(q, dsig + static_cast<uint64_t>(r) * N, N, c->Wp, planes + static_cast<uint64_t>(r) * 16 * 4 * c->Wp));
-  step(cudaEventRecord(ev[1], q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "event record failed"));
-  step(launch_fused_filter(q, query, data, R, qsig, planes, c));
-  step(cudaEventRecord(ev[2], q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "event record failed"));
-  step(launch_gmcr(q, query, data, c, m, true, 0));
-  step(cudaEventRecord(ev[3], q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "event record failed"));
-  if (!rc && cudaMemsetAsync(d_total, 0, 8, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
-  const bool exact = q->opts.profile == kProfileExact;
-  if (!exact) step(launch_join_literal(q, query, data, c, m, find_first, 0, std::min(data->low_offset_graphs, data->num_graphs), d_total));
-  step(launch_join_fast(q, query, data, c, m, find_first, d_total));
-  step(cudaEventRecord(ev[4], q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "event record failed"));
-  if (!rc) {
-    cudaError_t e = cudaMemcpyAsync(q->pinned, d_total, 8, cudaMemcpyDeviceToHost, q->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(q->stream);
-    if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "batched read-back failed: %s", cudaGetErrorString(e));
-  }
-  if (!rc) {
-    out->total_matches = *static_cast<uint64_t*>(q->pinned);
-    out->admitted_pairs = m->total;
-    out->pairs = static_cast<uint64_t>(query->num_graphs) * data->num_graphs;
-    float f;
-    cudaEventElapsedTime(&f, ev[0], ev[1]);
-    out->ms_signatures = f;
-    cudaEventElapsedTime(&f, ev[1], ev[2]);
-    out->ms_filter = f;
-    cudaEventElapsedTime(&f, ev[2], ev[3]);
-    out->ms_mapping = f;
-    cudaEventElapsedTime(&f, ev[3], ev[4]);
-    out->ms_join = f;
-    cudaEventElapsedTime(&f, ev[0], ev[4]);
-    out->ms_total = f;
-    m->counts_valid = true;
-  }
-  dev_free(q, buf);
   return rc;
 }
 

@@ -1,0 +1,272 @@
+// The batched form (sigmo_match_batched): signatures for all iterations in
+// one BFS, per-graph candidate planes, GMCR from the plane AND-programs, and
+// the persistent join, with one host synchronisation (the admitted-pair
+// total, as in gmcr.hpp:80) between the launches.  Results are identical to
+// the stage-per-launch calls (library/src/sigmo.cpp:98-160).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "internal.hpp"
+
+namespace sigmo_b200 {
+namespace {
+
+void free_program(Queue* q, PlaneProgram* pp) {
+  dev_free(q, pp->spec);
+  dev_free(q, pp->prog_off);
+  dev_free(q, pp->prog);
+  dev_free(q, pp->cls);
+  dev_free(q, pp->qsig_all);
+  *pp = PlaneProgram{};
+}
+
+int upload(Queue* q, void** dst, const void* src, size_t bytes) {
+  SIGMO_TRY(dev_alloc(q, dst, bytes ? bytes : 4));
+  if (bytes) SIGMO_CUDA_TRY(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, q->stream));
+  return SIGMO_OK;
+}
+
+}  // namespace
+
+// Builds (or reuses) the plane program of a query batch for R iterations:
+// query signatures of iterations 1..R on the device, then on the host the
+// distinct labels and (r, l, c) thresholds (the planes), the classes of
+// identical (label, signature_1..R) vertices, and each class's program
+// (label plane first, then its thresholds).
+int build_plane_program(Queue* q, Graph* query, uint32_t R) {
+  PlaneProgram& pp = query->pp;
+  if (pp.valid && pp.R == R && pp.profile == q->opts.profile) return SIGMO_OK;
+  free_program(q, &pp);
+  const uint64_t Qn = query->total_nodes;
+  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&pp.qsig_all), 8ull * (R ? R : 1) * (Qn ? Qn : 1)));
+  SIGMO_TRY(launch_sig_all(q, query, R, pp.qsig_all));
+  std::vector<uint64_t> sig(static_cast<size_t>(R) * Qn);
+  std::vector<uint8_t> lab(Qn);
+  if (Qn) {
+    if (R) SIGMO_CUDA_TRY(cudaMemcpyAsync(sig.data(), pp.qsig_all, 8ull * R * Qn, cudaMemcpyDeviceToHost, q->stream));
+    SIGMO_CUDA_TRY(cudaMemcpyAsync(lab.data(), query->node_labels, Qn, cudaMemcpyDeviceToHost, q->stream));
+  }
+  SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));
+
+  // planes: label values used by queries, then thresholds (r, l, c)
+  std::map<uint32_t, uint32_t> label_plane;
+  std::map<uint32_t, uint32_t> ge_plane;  // key r<<16 | l<<8 | c
+  for (uint64_t v = 0; v < Qn; ++v) label_plane[lab[v]] = 0;
+  for (uint32_t r = 0; r < R; ++r)
+    for (uint64_t v = 0; v < Qn; ++v) {
+      const uint64_t s = sig[r * Qn + v];
+      for (uint32_t l = 0; l < 16; ++l) {
+        const uint32_t c = sig_get(s, l);
+        if (c) ge_plane[(r << 16) | (l << 8) | c] = 0;
+      }
+    }
+  std::vector<uint32_t> spec;
+  for (auto& kv : label_plane) {
+    kv.second = static_cast<uint32_t>(spec.size());
+    spec.push_back(0x80000000u | kv.first);
+  }
+  for (auto& kv : ge_plane) {
+    kv.second = static_cast<uint32_t>(spec.size());
+    spec.push_back(kv.first);
+  }
+  if (spec.size() >= 65535) return fail(SIGMO_ERR_DOMAIN, "query batch needs %zu candidate planes (limit 65535)", spec.size());
+
+  // classes and programs
+  std::map<std::vector<uint64_t>, uint32_t> classes;
+  std::vector<uint32_t> cls(Qn), prog_off{0};
+  std::vector<uint16_t> prog;
+  std::vector<uint64_t> key(R + 1);
+  for (uint64_t v = 0; v < Qn; ++v) {
+    key[0] = lab[v];
+    for (uint32_t r = 0; r < R; ++r) key[r + 1] = sig[r * Qn + v];
+    auto it = classes.find(key);
+    if (it == classes.end()) {
+      const uint32_t id = static_cast<uint32_t>(classes.size());
+      it = classes.emplace(key, id).first;
+      prog.push_back(static_cast<uint16_t>(label_plane[lab[v]]));
+      for (uint32_t r = 0; r < R; ++r)
+        for (uint32_t l = 0; l < 16; ++l) {
+          const uint32_t c = sig_get(key[r + 1], l);
+          if (c) prog.push_back(static_cast<uint16_t>(ge_plane[(r << 16) | (l << 8) | c]));
+        }
+      prog_off.push_back(static_cast<uint32_t>(prog.size()));
+    }
+    cls[v] = it->second;
+  }
+  pp.K = static_cast<uint32_t>(spec.size());
+  pp.C = static_cast<uint32_t>(classes.size());
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.spec), spec.data(), 4 * spec.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog_off), prog_off.data(), 4 * prog_off.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog), prog.data(), 2 * prog.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.cls), cls.data(), 4 * cls.size()));
+  SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
+  pp.R = R;
+  pp.profile = q->opts.profile;
+  pp.valid = true;
+  return SIGMO_OK;
+}
+
+void release_plane_program(Graph* g) {
+  if (g->pp.valid || g->pp.qsig_all) free_program(g->q, &g->pp);
+}
+
+}  // namespace sigmo_b200
+
+using namespace sigmo_b200;
+
+namespace {
+
+struct Events {
+  cudaEvent_t e[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  ~Events() {
+    for (auto& x : e)
+      if (x) cudaEventDestroy(x);
+  }
+};
+
+// The bitset route: fused filter writes the final bitset (all words), GMCR
+// and the join read it.  Used when the caller asks for the bitset, or when a
+// batch does not fit the plane route.
+int batched_bitset(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, Candidates* c, Gmcr* m,
+                   uint64_t* d_total, Events& ev) {
+  PlaneProgram& pp = query->pp;
+  const uint64_t N = data->total_nodes;
+  void* buf = nullptr;
+  const uint64_t b_dsig = 8ull * R * N, b_planes = 16ull * 16 * R * c->Wp;
+  auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+  SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + 256));
+  uint64_t* dsig = static_cast<uint64_t*>(buf);
+  uint32_t* planes = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + al(b_dsig));
+  int rc = launch_sig_all(q, data, R, dsig);
+  for (uint32_t r = 0; r < R && !rc; ++r)
+    rc = launch_sig_planes(q, dsig + static_cast<uint64_t>(r) * N, N, c->Wp, planes + static_cast<uint64_t>(r) * 16 * 4 * c->Wp);
+  if (!rc && cudaEventRecord(ev.e[1], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc) rc = launch_fused_filter(q, query, data, R, pp.qsig_all, planes, c);
+  if (!rc && cudaEventRecord(ev.e[2], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc) rc = launch_gmcr(q, query, data, c, m, true, 0);
+  if (!rc && cudaEventRecord(ev.e[3], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  const bool exact = q->opts.profile == kProfileExact;
+  if (!rc && !exact) rc = launch_join_literal(q, query, data, c, m, find_first, 0, std::min(data->low_offset_graphs, data->num_graphs), d_total);
+  if (!rc) rc = launch_join_fast(q, query, data, c, m, find_first, d_total);
+  dev_free(q, buf);
+  return rc;
+}
+
+// The plane route (no full bitset in HBM).
+int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, Gmcr* m, uint64_t* d_total, Events& ev) {
+  PlaneProgram& pp = query->pp;
+  const uint64_t N = data->total_nodes, Qn = query->total_nodes;
+  const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, AW = data->adj_words;
+  const bool exact = q->opts.profile == kProfileExact;
+  const uint32_t L = exact ? 0u : std::min(data->low_offset_graphs, G);
+  // words of the bitset the literal join reads (graphs [0, L))
+  const uint64_t Wlow = L ? (static_cast<uint64_t>(data->host_graph_offsets[L]) + 31) / 32 : 0;
+  const uint64_t Wlp = (Wlow + 31) / 32 * 32;
+  auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+  const uint64_t b_dsig = 8ull * R * N, b_planes = 8ull * GW * pp.K * AW * 32, b_ne = 4ull * pp.C * GW;
+  const uint64_t b_lplanes = 16ull * 16 * R * Wlp, b_lbits = 4ull * Qn * Wlp;
+  void* buf = nullptr;
+  SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + al(b_ne) + al(b_lplanes) + al(b_lbits) + 256));
+  char* p = static_cast<char*>(buf);
+  uint64_t* dsig = reinterpret_cast<uint64_t*>(p);
+  p += al(b_dsig);
+  uint64_t* planes = reinterpret_cast<uint64_t*>(p);
+  p += al(b_planes);
+  uint32_t* NE = reinterpret_cast<uint32_t*>(p);
+  p += al(b_ne);
+  uint32_t* lplanes = reinterpret_cast<uint32_t*>(p);
+  p += al(b_lplanes);
+  uint32_t* lbits = reinterpret_cast<uint32_t*>(p);
+  int rc = launch_sig_all(q, data, R, dsig);
+  if (!rc && b_planes && cudaMemsetAsync(planes, 0, b_planes, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
+  if (!rc) rc = launch_build_planes(q, data, dsig, R, pp, planes);
+  if (!rc && cudaEventRecord(ev.e[1], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc) rc = launch_ne_planes(q, data, pp, planes, NE);
+  if (!rc && cudaEventRecord(ev.e[2], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc) rc = launch_gmcr_from_ne(q, query, data, NE, pp.cls, m, true, 0);
+  if (!rc && cudaEventRecord(ev.e[3], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc && L && m->total) {
+    // REF_PTX: graphs starting below vertex 256 keep the reference's live
+    // `visited` bitset, so they take the literal join on the bitset words it reads.
+    for (uint32_t r = 0; r < R && !rc; ++r)
+      rc = launch_sig_planes(q, dsig + static_cast<uint64_t>(r) * N, N, Wlp, lplanes + static_cast<uint64_t>(r) * 16 * 4 * Wlp);
+    if (!rc) rc = launch_fused_filter_raw(q, query->node_labels, pp.qsig_all, Qn, data->node_labels, N, lplanes, Wlp, R, lbits);
+    Candidates view;
+    view.q = q;
+    view.rows = Qn;
+    view.targets = N;
+    view.W = Wlow;
+    view.Wp = Wlp;
+    view.bits = lbits;
+    if (!rc) rc = launch_join_literal(q, query, data, &view, m, find_first, 0, L, d_total);
+  }
+  if (!rc) rc = launch_join_fast_planes(q, query, data, pp, planes, m, find_first, d_total);
+  dev_free(q, buf);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t R, int find_first,
+                                   uint32_t flags, sigmo_candidates_t c, sigmo_gmcr_t m, sigmo_match_result* out) {
+  if (!q || !query || !data || !m || !out) return fail(SIGMO_ERR_INVALID, "null argument");
+  const bool materialize = (flags & SIGMO_MATCH_MATERIALIZE_BITSET) != 0;
+  if (materialize && !c) return fail(SIGMO_ERR_INVALID, "SIGMO_MATCH_MATERIALIZE_BITSET needs a candidates object");
+  if (c && (c->rows != query->total_nodes || c->targets != data->total_nodes))
+    return fail(SIGMO_ERR_INVALID, "candidate bitset does not match the graphs");
+  if (m->q != q || (c && c->q != q) || query->q != q || data->q != q) return fail(SIGMO_ERR_INVALID, "handles belong to another queue");
+  if (query->max_nodes > kMaxQueryNodes)
+    return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
+  if (data->max_nodes > 64u * kMaxAdjWords)
+    return fail(SIGMO_ERR_DOMAIN, "the batched form supports data graphs of up to %u vertices (largest: %u)", 64u * kMaxAdjWords,
+                data->max_nodes);
+  SIGMO_CUDA_TRY(cudaSetDevice(q->device));
+  std::memset(out, 0, sizeof(*out));
+  Events ev;
+  for (auto& e : ev.e) SIGMO_CUDA_TRY(cudaEventCreate(&e));
+  SIGMO_CUDA_TRY(cudaEventRecord(ev.e[0], q->stream));
+  SIGMO_TRY(build_plane_program(q, query, R));
+  uint64_t* d_total = nullptr;
+  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
+  int rc = cudaMemsetAsync(d_total, 0, 8, q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "memset failed");
+  const bool planes_fit = ne_planes_smem(query->pp.K, data->adj_words) <= 200u * 1024u;
+  if (!rc) {
+    if (materialize || !planes_fit) {
+      sigmo_candidates_t cc = c;
+      if (!cc) rc = sigmo_candidates_create(q, query->total_nodes, data->total_nodes, &cc);
+      if (!rc) rc = batched_bitset(q, query, data, R, find_first, cc, m, d_total, ev);
+      if (cc != c) sigmo_candidates_destroy(cc);
+    } else {
+      rc = batched_planes(q, query, data, R, find_first, m, d_total, ev);
+    }
+  }
+  if (!rc && cudaEventRecord(ev.e[4], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc) {
+    cudaError_t e = cudaMemcpyAsync(q->pinned, d_total, 8, cudaMemcpyDeviceToHost, q->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(q->stream);
+    if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "batched read-back failed: %s", cudaGetErrorString(e));
+  }
+  if (!rc) {
+    out->total_matches = *static_cast<uint64_t*>(q->pinned);
+    out->admitted_pairs = m->total;
+    out->pairs = static_cast<uint64_t>(query->num_graphs) * data->num_graphs;
+    float f;
+    cudaEventElapsedTime(&f, ev.e[0], ev.e[1]);
+    out->ms_signatures = f;
+    cudaEventElapsedTime(&f, ev.e[1], ev.e[2]);
+    out->ms_filter = f;
+    cudaEventElapsedTime(&f, ev.e[2], ev.e[3]);
+    out->ms_mapping = f;
+    cudaEventElapsedTime(&f, ev.e[3], ev.e[4]);
+    out->ms_join = f;
+    cudaEventElapsedTime(&f, ev.e[0], ev.e[4]);
+    out->ms_total = f;
+    m->counts_valid = true;
+  }
+  dev_free(q, d_total);
+  return rc;
+}

@@ -39,6 +39,20 @@ struct Queue {
   void* pinned = nullptr;  // small pinned host buffer for scalar read-backs
 };
 
+// Per-query-batch plane program of the batched form (kernels_planes.cu).
+struct PlaneProgram {
+  bool valid = false;
+  uint32_t R = 0;
+  int profile = 0;
+  uint32_t K = 0;                 // planes per data graph
+  uint32_t C = 0;                 // classes of identical query vertices
+  uint32_t* spec = nullptr;       // [K] plane definitions
+  uint32_t* prog_off = nullptr;   // [C + 1]
+  uint16_t* prog = nullptr;       // plane indices of each class's program
+  uint32_t* cls = nullptr;        // [query vertices] class of each vertex
+  uint64_t* qsig_all = nullptr;   // [R][query vertices] signatures, iterations 1..R
+};
+
 struct Graph {
   Queue* q = nullptr;
   bool owned = true;
@@ -61,6 +75,7 @@ struct Graph {
   uint64_t* qsel = nullptr;        // [total_nodes] adjacency to earlier levels
   uint64_t* qsel_id = nullptr;     // [total_nodes] same, identity order
   std::vector<uint32_t> host_graph_offsets;  // host copy (sizes, dispatch)
+  PlaneProgram pp;                 // when this graph is the query side of a batched match
 };
 
 struct Candidates {
@@ -134,7 +149,19 @@ int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const C
                         uint32_t graph_begin, uint32_t graph_end, uint64_t* d_total);
 int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
                      uint64_t* d_total);
+int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, const PlaneProgram& pp, const uint64_t* planes,
+                            Gmcr* m, int find_first, uint64_t* d_total);
+int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const uint32_t* NE, const uint32_t* cls, Gmcr* m,
+                        bool sync_total, uint64_t capacity_hint);
+int launch_build_planes(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
+                        uint64_t* planes);
+int launch_ne_planes(Queue* q, const Graph* data, const PlaneProgram& pp, const uint64_t* planes, uint32_t* NE);
+size_t ne_planes_smem(uint32_t K, uint32_t AW);
+int launch_fused_filter_raw(Queue* q, const uint8_t* qlab, const uint64_t* qsig_all, uint64_t Qn, const uint8_t* dlab,
+                            uint64_t N, const uint32_t* planes_all, uint64_t Wstride, uint32_t R, uint32_t* bits);
 int launch_row_counts(Queue* q, const Candidates* c, uint32_t* d_counts);
+int build_plane_program(Queue* q, Graph* query, uint32_t R);
+void release_plane_program(Graph* g);
 int launch_digest(Queue* q, const Candidates* c, uint64_t* d_digest);
 
 }  // namespace sigmo_b200

@@ -246,6 +246,19 @@ int launch_fused_filter(Queue* q, const Graph* query, const Graph* data, uint32_
   return check_launch(q, "k_fused_filter");
 }
 
+// Fused filter over the first `Wstride` words of every row into a bitset of
+// that row stride (the batched form materialises only the words its literal
+// join reads).
+int launch_fused_filter_raw(Queue* q, const uint8_t* qlab, const uint64_t* qsig_all, uint64_t Qn, const uint8_t* dlab,
+                            uint64_t N, const uint32_t* planes_all, uint64_t Wstride, uint32_t R, uint32_t* bits) {
+  if (!Qn || !Wstride) return SIGMO_OK;
+  dim3 grid(grid_for(Wstride, kWordsPerBlock), static_cast<unsigned>((Qn + kRowsPerBlock - 1) / kRowsPerBlock));
+  if (grid.y > 65535u) return fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", (unsigned long long)Qn);
+  k_fused_filter<<<grid, kWordsPerBlock, 0, q->stream>>>(qlab, qsig_all, Qn, dlab, N, reinterpret_cast<const uint4*>(planes_all),
+                                                         Wstride, R, bits);
+  return check_launch(q, "k_fused_filter");
+}
+
 int launch_row_counts(Queue* q, const Candidates* c, uint32_t* d_counts) {
   if (!c->rows) return SIGMO_OK;
   k_row_counts<<<grid_for(c->rows, 1, 148u * 64u), 256, 0, q->stream>>>(c->bits, c->rows, c->W, c->Wp, d_counts);

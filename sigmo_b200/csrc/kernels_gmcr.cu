@@ -49,8 +49,11 @@ __global__ void k_gmcr_ne(const uint32_t* __restrict__ bits, uint64_t Wp, uint64
 }
 
 // Warp per 32 data graphs; lanes take query graphs 32 at a time.
+// NE rows are indexed by query vertex, or by the vertex's class when cls is
+// given (the batched form stores one row per class of identical vertices).
 __global__ void k_gmcr_admit(const uint32_t* __restrict__ NE, uint32_t GW, const uint32_t* __restrict__ qgoff, uint32_t QG,
-                             uint32_t G, uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
+                             uint32_t G, const uint32_t* __restrict__ cls, uint32_t* __restrict__ admit,
+                             uint32_t* __restrict__ counts) {
   const unsigned lane = threadIdx.x & 31u;
   const uint32_t warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
@@ -64,7 +67,10 @@ __global__ void k_gmcr_admit(const uint32_t* __restrict__ NE, uint32_t GW, const
         const uint32_t off = qgoff[q], n = qgoff[q + 1] - off;
         if (n > 1) {
           a = valid;
-          for (uint32_t j = 0; j < n && a; ++j) a &= NE[static_cast<uint64_t>(off + j) * GW + gw];
+          for (uint32_t j = 0; j < n && a; ++j) {
+            const uint32_t row = cls ? cls[off + j] : off + j;
+            a &= NE[static_cast<uint64_t>(row) * GW + gw];
+          }
         }
         admit[static_cast<uint64_t>(q) * GW + gw] = a;
       }
@@ -106,14 +112,14 @@ __global__ void k_gmcr_fill(const uint32_t* __restrict__ admit, uint32_t GW, uin
 
 }  // namespace
 
-// Builds m->offsets / indices / pair_graph.  With sync_total the total is read
-// back and the index arrays sized exactly (the reference reads it back too,
+// Admission, counts, scan and fill from an NE matrix (rows per query vertex,
+// or per class when cls != nullptr).  With sync_total the total is read back
+// and the index arrays sized exactly (the reference reads it back too,
 // gmcr.hpp:80); otherwise capacity_hint bounds them.
-int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, bool sync_total,
-                uint64_t capacity_hint) {
+int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const uint32_t* NE, const uint32_t* cls, Gmcr* m,
+                        bool sync_total, uint64_t capacity_hint) {
   const uint32_t G = data->num_graphs, QG = query->num_graphs;
   const uint32_t GW = (G + 31u) / 32u;
-  const uint64_t Qn = query->total_nodes;
   if (m->offsets && m->num_data_graphs != G) {
     dev_free(q, m->offsets);
     m->offsets = nullptr;
@@ -122,47 +128,39 @@ int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidate
   m->num_data_graphs = G;
   m->counts_valid = false;
   SIGMO_CUDA_TRY(cudaMemsetAsync(m->offsets, 0, sizeof(uint32_t) * (G + 1ull), q->stream));
-
-  // scratch: NE [Qn][GW], admit [QG][GW], counts [G], cub temp
-  const uint64_t ne_words = Qn * GW, admit_words = static_cast<uint64_t>(QG) * GW;
+  const uint64_t admit_words = static_cast<uint64_t>(QG) * GW;
   size_t cub_bytes = 0;
   if (G) cub::DeviceScan::InclusiveSum(nullptr, cub_bytes, static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
                                        static_cast<int>(G), q->stream);
   auto al = [](size_t x) { return (x + 255) & ~static_cast<size_t>(255); };
-  const size_t bytes = al(ne_words * 4) + al(admit_words * 4) + al(G * 4ull) + al(cub_bytes) + 256;
-  void* scratch = nullptr;
-  SIGMO_TRY(queue_scratch(q, bytes, &scratch));
-  char* p = static_cast<char*>(scratch);
-  uint32_t* NE = reinterpret_cast<uint32_t*>(p);
-  p += al(ne_words * 4);
+  void* buf = nullptr;
+  SIGMO_TRY(dev_alloc(q, &buf, al(admit_words * 4) + al(G * 4ull) + al(cub_bytes) + 256));
+  char* p = static_cast<char*>(buf);
   uint32_t* admit = reinterpret_cast<uint32_t*>(p);
   p += al(admit_words * 4);
   uint32_t* counts = reinterpret_cast<uint32_t*>(p);
   p += al(G * 4ull);
   void* cub_tmp = p;
-
-  if (G && QG && Qn) {
-    dim3 grid_ne((GW + 7u) / 8u, static_cast<unsigned>((Qn + kNeRowsPerBlock - 1) / kNeRowsPerBlock));
-    if (grid_ne.y > 65535u) return fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", (unsigned long long)Qn);
-    k_gmcr_ne<<<grid_ne, 256, 0, q->stream>>>(c->bits, c->Wp, Qn, data->graph_offsets, G, GW, q->opts.profile, NE);
-    SIGMO_TRY(check_launch(q, "k_gmcr_ne"));
-    k_gmcr_admit<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(NE, GW, query->graph_offsets, QG, G, admit, counts);
-    SIGMO_TRY(check_launch(q, "k_gmcr_admit"));
-    SIGMO_CUDA_TRY(cub::DeviceScan::InclusiveSum(cub_tmp, cub_bytes, counts, m->offsets + 1, static_cast<int>(G), q->stream));
-    q->launches++;
+  int rc = SIGMO_OK;
+  if (G && QG) {
+    k_gmcr_admit<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(NE, GW, query->graph_offsets, QG, G, cls, admit, counts);
+    rc = check_launch(q, "k_gmcr_admit");
+    if (!rc) {
+      cudaError_t e = cub::DeviceScan::InclusiveSum(cub_tmp, cub_bytes, counts, m->offsets + 1, static_cast<int>(G), q->stream);
+      if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "device scan failed: %s", cudaGetErrorString(e));
+      q->launches += 2;
+    }
   }
-
-  uint64_t cap;
-  if (sync_total) {
+  uint64_t cap = capacity_hint;
+  if (!rc && sync_total) {
     uint32_t* pinned = static_cast<uint32_t*>(q->pinned);
-    SIGMO_CUDA_TRY(cudaMemcpyAsync(pinned, m->offsets + G, sizeof(uint32_t), cudaMemcpyDeviceToHost, q->stream));
-    SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));
+    cudaError_t e = cudaMemcpyAsync(pinned, m->offsets + G, sizeof(uint32_t), cudaMemcpyDeviceToHost, q->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(q->stream);
+    if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "reading the GMCR total failed: %s", cudaGetErrorString(e));
     m->total = *pinned;
     cap = m->total;
-  } else {
-    cap = capacity_hint;
   }
-  if (cap > m->capacity || !m->indices) {
+  if (!rc && (cap > m->capacity || !m->indices)) {
     dev_free(q, m->indices);
     dev_free(q, m->pair_graph);
     dev_free(q, m->counts);
@@ -170,17 +168,41 @@ int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidate
     m->counts = nullptr;
     m->capacity = 0;
     const uint64_t n = cap ? cap : 1;
-    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&m->indices), sizeof(uint32_t) * n));
-    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&m->pair_graph), sizeof(uint32_t) * n));
-    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&m->counts), sizeof(uint64_t) * n));
-    m->capacity = cap;
+    rc = dev_alloc(q, reinterpret_cast<void**>(&m->indices), sizeof(uint32_t) * n);
+    if (!rc) rc = dev_alloc(q, reinterpret_cast<void**>(&m->pair_graph), sizeof(uint32_t) * n);
+    if (!rc) rc = dev_alloc(q, reinterpret_cast<void**>(&m->counts), sizeof(uint64_t) * n);
+    if (!rc) m->capacity = cap;
   }
-  if (G && QG && Qn) {
+  if (!rc && G && QG) {
     k_gmcr_fill<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(admit, GW, QG, G, m->offsets, m->indices,
                                                                                 m->pair_graph, m->capacity);
-    SIGMO_TRY(check_launch(q, "k_gmcr_fill"));
+    rc = check_launch(q, "k_gmcr_fill");
   }
-  return SIGMO_OK;
+  dev_free(q, buf);
+  return rc;
+}
+
+// GMCR from the candidate bitset: NE per query vertex, then the above.
+int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, bool sync_total,
+                uint64_t capacity_hint) {
+  const uint32_t G = data->num_graphs;
+  const uint32_t GW = (G + 31u) / 32u;
+  const uint64_t Qn = query->total_nodes;
+  void* ne = nullptr;
+  SIGMO_TRY(dev_alloc(q, &ne, 4ull * Qn * GW + 4));
+  uint32_t* NE = static_cast<uint32_t*>(ne);
+  int rc = SIGMO_OK;
+  if (G && query->num_graphs && Qn) {
+    dim3 grid_ne((GW + 7u) / 8u, static_cast<unsigned>((Qn + kNeRowsPerBlock - 1) / kNeRowsPerBlock));
+    if (grid_ne.y > 65535u) rc = fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", (unsigned long long)Qn);
+    if (!rc) {
+      k_gmcr_ne<<<grid_ne, 256, 0, q->stream>>>(c->bits, c->Wp, Qn, data->graph_offsets, G, GW, q->opts.profile, NE);
+      rc = check_launch(q, "k_gmcr_ne");
+    }
+  }
+  if (!rc) rc = launch_gmcr_from_ne(q, query, data, NE, nullptr, m, sync_total, capacity_hint);
+  dev_free(q, ne);
+  return rc;
 }
 
 }  // namespace sigmo_b200

@@ -213,9 +213,28 @@ __device__ __forceinline__ void extract_local(const uint32_t* __restrict__ row, 
   }
 }
 
-template <int AW, bool EXACT>
+// Candidate set of query vertex v (global id) in data graph g from the plane
+// tiles: the AND of the planes of v's class program.
+template <int AW>
+__device__ __forceinline__ void mask_from_planes(const uint64_t* __restrict__ planes, uint32_t K, uint32_t g, uint32_t cls_v,
+                                                 const uint32_t* __restrict__ prog_off, const uint16_t* __restrict__ prog,
+                                                 uint64_t* out) {
+  const uint64_t* base = planes + static_cast<uint64_t>(g >> 5) * K * AW * 32 + (g & 31u);
+#pragma unroll
+  for (int w = 0; w < AW; ++w) out[w] = ~0ull;
+  const uint32_t e1 = prog_off[cls_v + 1];
+  for (uint32_t e = prog_off[cls_v]; e < e1; ++e) {
+    const uint32_t k = prog[e];
+#pragma unroll
+    for (int w = 0; w < AW; ++w) out[w] &= base[(static_cast<uint64_t>(k) * AW + w) * 32];
+  }
+}
+
+template <int AW, bool EXACT, bool FROM_PLANES>
 __global__ void __launch_bounds__(128) k_join_fast(
-    const uint32_t* __restrict__ bits, uint64_t Wp, int prof, const uint32_t* __restrict__ qgoff,
+    const uint32_t* __restrict__ bits, uint64_t Wp, const uint64_t* __restrict__ planes, uint32_t K,
+    const uint32_t* __restrict__ prog_off, const uint16_t* __restrict__ prog, const uint32_t* __restrict__ cls,
+    int prof, const uint32_t* __restrict__ qgoff,
     const uint8_t* __restrict__ qorder, const uint64_t* __restrict__ qsel, const uint64_t* __restrict__ qsel_id,
     const uint8_t* __restrict__ qsym, const uint32_t* __restrict__ dgoff, const uint64_t* __restrict__ dadj,
     const uint8_t* __restrict__ dsym, const uint32_t* __restrict__ indices, const uint32_t* __restrict__ pair_graph,
@@ -245,7 +264,8 @@ __global__ void __launch_bounds__(128) k_join_fast(
       const uint64_t* selp = (ident ? qsel_id : qsel) + qoff;
       for (uint32_t k = 0; k < n; ++k) {
         const uint32_t v = ident ? k : qorder[qoff + k];
-        extract_local<AW>(bits + static_cast<uint64_t>(qoff + v) * Wp, s, e, prof, M[k]);
+        if (FROM_PLANES) mask_from_planes<AW>(planes, K, g, cls[qoff + v], prog_off, prog, M[k]);
+        else extract_local<AW>(bits + static_cast<uint64_t>(qoff + v) * Wp, s, e, prof, M[k]);
       }
 #pragma unroll
       for (int w = 0; w < AW; ++w) cand[0][w] = M[0][w];
@@ -355,7 +375,8 @@ int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Cand
   const unsigned grid = grid_for((m->total + 31) / 32 * 32, block, 148u * 16u);
   auto* tot = reinterpret_cast<unsigned long long*>(d_total);
 #define SIGMO_JOIN_FAST(AWV, EX)                                                                                    \
-  k_join_fast<AWV, EX><<<grid, block, 0, q->stream>>>(c->bits, c->Wp, q->opts.profile, query->graph_offsets, query->qorder, \
+  k_join_fast<AWV, EX, false><<<grid, block, 0, q->stream>>>(c->bits, c->Wp, nullptr, 0, nullptr, nullptr, nullptr,         \
+                                                       q->opts.profile, query->graph_offsets, query->qorder,             \
                                                        query->qsel, query->qsel_id, query->sym, data->graph_offsets,     \
                                                        data->adj, data->sym, m->indices, m->pair_graph, m->total, skip,  \
                                                        find_first, cursor, m->counts, tot)
@@ -366,6 +387,38 @@ int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Cand
   }
 #undef SIGMO_JOIN_FAST
   return check_launch(q, "k_join_fast");
+}
+
+int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, const PlaneProgram& pp, const uint64_t* planes,
+                            Gmcr* m, int find_first, uint64_t* d_total) {
+  if (!m->total) return SIGMO_OK;
+  if (query->max_nodes > kMaxQueryNodes)
+    return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
+  const bool exact = q->opts.profile == kProfileExact;
+  SIGMO_TRY(launch_query_order(const_cast<Graph*>(query)));
+  void* cur = nullptr;
+  SIGMO_TRY(dev_alloc(q, &cur, 256));
+  auto* cursor = static_cast<unsigned long long*>(cur);
+  SIGMO_CUDA_TRY(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), q->stream));
+  const uint32_t skip = exact ? 0u : data->low_offset_graphs;
+  const unsigned block = 128;
+  const unsigned grid = grid_for((m->total + 31) / 32 * 32, block, 148u * 16u);
+  auto* tot = reinterpret_cast<unsigned long long*>(d_total);
+#define SIGMO_JOIN_PLANES(AWV, EX)                                                                                      \
+  k_join_fast<AWV, EX, true><<<grid, block, 0, q->stream>>>(nullptr, 0, planes, pp.K, pp.prog_off, pp.prog, pp.cls,      \
+                                                            q->opts.profile, query->graph_offsets, query->qorder,        \
+                                                            query->qsel, query->qsel_id, query->sym, data->graph_offsets, \
+                                                            data->adj, data->sym, m->indices, m->pair_graph, m->total,   \
+                                                            skip, find_first, cursor, m->counts, tot)
+  switch (data->adj_words) {
+    case 1: if (exact) SIGMO_JOIN_PLANES(1, true); else SIGMO_JOIN_PLANES(1, false); break;
+    case 2: if (exact) SIGMO_JOIN_PLANES(2, true); else SIGMO_JOIN_PLANES(2, false); break;
+    default: if (exact) SIGMO_JOIN_PLANES(4, true); else SIGMO_JOIN_PLANES(4, false); break;
+  }
+#undef SIGMO_JOIN_PLANES
+  int rc = check_launch(q, "k_join_fast<planes>");
+  dev_free(q, cur);
+  return rc;
 }
 
 }  // namespace sigmo_b200

@@ -49,14 +49,22 @@ def run_plain(qh, dh, R, profile, find_first, wg=128, keep=False):
 
 
 def run_batched(qh, dh, R, profile, find_first, wg=128, keep_bits=False):
+    """keep_bits: the bitset route (final bitset materialised); otherwise the
+    plane route, which never writes the bitset."""
     queue = sb.Queue(0, profile=profile, join_work_group_size=wg)
     qg, dg = sb.createDeviceCSRGraph(queue, qh), sb.createDeviceCSRGraph(queue, dh)
-    cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes)
+    cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes) if keep_bits else None
     gm = sb.GMCR(queue)
-    res = sb.match_batched(queue, qg, dg, R, find_first, cand, gm)
+    res = sb.match_batched(queue, qg, dg, R, find_first, cand, gm, materialize=keep_bits)
     off, idx = gm.getGMCR()
     return {"offsets": off, "indices": idx, "per_pair": gm.getPairCounts(), "total": res["total_matches"],
-            "digest": cand.digest(), "final": cand.getHostCandidates() if keep_bits else None, "res": res}
+            "digest": cand.digest() if keep_bits else None, "final": cand.getHostCandidates() if keep_bits else None,
+            "res": res}
+
+
+def run_both_batched(qh, dh, R, profile, find_first, wg=128):
+    return [run_batched(qh, dh, R, profile, find_first, wg, keep_bits=False),
+            run_batched(qh, dh, R, profile, find_first, wg, keep_bits=True)]
 
 
 @pytest.fixture(scope="module")
@@ -99,12 +107,13 @@ def test_batched_form_matches_golden(golden):
         R, prof = run["iterations"], run["profile"]
         ctx = f"{case['name']} profile={prof} R={R}"
         for ff, key in ((False, "all"), (True, "first")):
-            out = run_batched(qh, dh, R, prof, ff, keep_bits=True)
-            assert out["final"].tolist() == run["bitsets"][-1], ctx
-            assert out["offsets"].tolist() == run["offsets"], ctx
-            assert out["indices"].tolist() == run["indices"], ctx
-            assert out["per_pair"].tolist() == run[f"per_pair_{key}"], f"{ctx} {key}"
-            assert out["total"] == run[f"total_{key}"], f"{ctx} {key}"
+            for out in run_both_batched(qh, dh, R, prof, ff):
+                if out["final"] is not None:
+                    assert out["final"].tolist() == run["bitsets"][-1], ctx
+                assert out["offsets"].tolist() == run["offsets"], ctx
+                assert out["indices"].tolist() == run["indices"], ctx
+                assert out["per_pair"].tolist() == run[f"per_pair_{key}"], f"{ctx} {key}"
+                assert out["total"] == run[f"total_{key}"], f"{ctx} {key}"
 
 
 def _oracle(qh, dh, R, prof, ff, wg=128, keep=False):
@@ -112,11 +121,16 @@ def _oracle(qh, dh, R, prof, ff, wg=128, keep=False):
 
 
 def _check(out, ref, ctx):
+    if isinstance(out, list):
+        for o in out:
+            _check(o, ref, ctx)
+        return
     assert out["offsets"].tolist() == ref["offsets"].tolist(), ctx
     assert out["indices"].tolist() == ref["indices"].tolist(), ctx
     assert np.array_equal(out["per_pair"], ref["per_pair"]), ctx
     assert out["total"] == ref["total"], ctx
-    assert out["digest"] == oracle.digest(ref["bits"]), ctx
+    if out["digest"] is not None:
+        assert out["digest"] == oracle.digest(ref["bits"]), ctx
 
 
 @pytest.mark.parametrize("prof", DEVICE_PROFILES)
@@ -133,10 +147,10 @@ def test_small_drug_like_config(prof):
         assert np.array_equal(out["sig_query"][it], ref["sig_query"][it]), it
         assert np.array_equal(out["bitsets"][it], ref["bitsets"][it]), it
     _check(out, ref, "plain find-all")
-    _check(run_batched(qh, dh, R, prof, False), ref, "batched find-all")
+    _check(run_both_batched(qh, dh, R, prof, False), ref, "batched find-all")
     ref1 = _oracle(qh, dh, R, prof, True)
     _check(run_plain(qh, dh, R, prof, True), ref1, "plain find-first")
-    _check(run_batched(qh, dh, R, prof, True), ref1, "batched find-first")
+    _check(run_both_batched(qh, dh, R, prof, True), ref1, "batched find-first")
     assert ref["total"] > 0 and len(ref["indices"]) > 0
 
 
@@ -147,7 +161,7 @@ def test_join_work_group_sizes(wg):
     qh = sb.generate_queries(300, 3, 8, seed=78)
     ref = _oracle(qh, dh, 2, oracle.REF_PTX, False, wg=wg)
     _check(run_plain(qh, dh, 2, oracle.REF_PTX, False, wg=wg), ref, f"plain wg={wg}")
-    _check(run_batched(qh, dh, 2, oracle.REF_PTX, False, wg=wg), ref, f"batched wg={wg}")
+    _check(run_both_batched(qh, dh, 2, oracle.REF_PTX, False, wg=wg), ref, f"batched wg={wg}")
 
 
 @pytest.mark.parametrize("prof", DEVICE_PROFILES)
@@ -161,7 +175,7 @@ def test_heavy_tail_graphs_over_64_atoms(prof):
         for it in range(R + 1):
             assert np.array_equal(out["bitsets"][it], ref["bitsets"][it]), (R, it)
         _check(out, ref, f"plain R={R}")
-        _check(run_batched(qh, dh, R, prof, False), ref, f"batched R={R}")
+        _check(run_both_batched(qh, dh, R, prof, False), ref, f"batched R={R}")
 
 
 @pytest.mark.parametrize("prof", DEVICE_PROFILES)
@@ -170,7 +184,7 @@ def test_symmetry_stress_small(prof):
     qh = sb.generate_queries(12, 4, 10, seed=42, kind=3)
     ref = _oracle(qh, dh, 3, prof, False)
     _check(run_plain(qh, dh, 3, prof, False), ref, "plain")
-    _check(run_batched(qh, dh, 3, prof, False), ref, "batched")
+    _check(run_both_batched(qh, dh, 3, prof, False), ref, "batched")
     assert ref["per_pair"].max() >= 12  # automorphic patterns give many embeddings
 
 
@@ -187,7 +201,7 @@ def test_edge_inputs():
             for ff in (False, True):
                 ref = _oracle(qh, dh, R, prof, ff)
                 _check(run_plain(qh, dh, R, prof, ff), ref, f"plain {prof} {R} {ff}")
-                _check(run_batched(qh, dh, R, prof, ff), ref, f"batched {prof} {R} {ff}")
+                _check(run_both_batched(qh, dh, R, prof, ff), ref, f"batched {prof} {R} {ff}")
 
 
 def test_graph_ending_on_word_boundary_masks():
@@ -202,7 +216,7 @@ def test_graph_ending_on_word_boundary_masks():
         ref = _oracle(qh, dh, 0, prof, False)
         out = run_plain(qh, dh, 0, prof, False)
         _check(out, ref, str(prof))
-        _check(run_batched(qh, dh, 0, prof, False), ref, str(prof))
+        _check(run_both_batched(qh, dh, 0, prof, False), ref, str(prof))
         outs[prof] = out
     assert outs[oracle.REF_PTX]["total"] != outs[oracle.EXACT]["total"]
 
@@ -227,5 +241,5 @@ def test_mid_size_slice_against_oracle():
     qh = sb.generate_queries(120, 3, 30, seed=2025, skew_lo=6, skew_hi=15)
     for ff in (False, True):
         ref = _oracle(qh, dh, 6, oracle.REF_PTX, ff)
-        _check(run_batched(qh, dh, 6, oracle.REF_PTX, ff), ref, f"batched ff={ff}")
+        _check(run_both_batched(qh, dh, 6, oracle.REF_PTX, ff), ref, f"batched ff={ff}")
         _check(run_plain(qh, dh, 6, oracle.REF_PTX, ff), ref, f"plain ff={ff}")
