@@ -117,6 +117,9 @@ int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out
   if (st == cudaSuccess) st = cudaEventCreate(&q->ev_start);
   if (st == cudaSuccess) st = cudaEventCreate(&q->ev_end);
   if (st == cudaSuccess) st = cudaMallocHost(&q->pinned, 4096);
+  if (st == cudaSuccess) st = cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking);
+  if (st == cudaSuccess) st = cudaEventCreateWithFlags(&q->ev_fork, cudaEventDisableTiming);
+  if (st == cudaSuccess) st = cudaEventCreateWithFlags(&q->ev_join, cudaEventDisableTiming);
   if (st == cudaSuccess) {
     // Keep freed stream-ordered allocations cached in the device's default pool
     // (per-call scratch is then reused instead of being remapped every call).
@@ -142,6 +145,12 @@ int sigmo_queue_destroy(sigmo_queue_t q) {
     cudaStreamSynchronize(q->stream);
     cudaStreamDestroy(q->stream);
   }
+  if (q->side) {
+    cudaStreamSynchronize(q->side);
+    cudaStreamDestroy(q->side);
+  }
+  if (q->ev_fork) cudaEventDestroy(q->ev_fork);
+  if (q->ev_join) cudaEventDestroy(q->ev_join);
   if (q->ev_start) cudaEventDestroy(q->ev_start);
   if (q->ev_end) cudaEventDestroy(q->ev_end);
   if (q->pinned) cudaFreeHost(q->pinned);
@@ -521,12 +530,12 @@ int sigmo_refine_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t 
   if (!s->data_planes || s->planes_Wp != c->Wp) {
     dev_free(q, s->data_planes);
     s->data_planes = nullptr;
-    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&s->data_planes), 16ull * 16 * c->Wp));
+    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&s->data_planes), 4ull * 16 * 15 * c->Wp));
     s->planes_Wp = c->Wp;
     s->planes_valid = false;
   }
   if (!s->planes_valid) {
-    SIGMO_TRY(launch_sig_planes(q, s->data_sig, s->data_nodes, c->Wp, s->data_planes));
+    SIGMO_TRY(launch_sig_thermo(q, s->data_sig, s->data_nodes, c->Wp, s->data_planes));
     s->planes_valid = true;
   }
   SIGMO_TRY(launch_refine(q, query, data, s->query_sig, s->data_planes, c));

@@ -20,6 +20,7 @@ void free_program(Queue* q, PlaneProgram* pp) {
   dev_free(q, pp->prog_off);
   dev_free(q, pp->prog);
   dev_free(q, pp->cls);
+  dev_free(q, pp->cp);
   dev_free(q, pp->qsig_all);
   *pp = PlaneProgram{};
 }
@@ -75,34 +76,50 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   }
   if (spec.size() >= 65535) return fail(SIGMO_ERR_DOMAIN, "query batch needs %zu candidate planes (limit 65535)", spec.size());
 
-  // classes and programs
-  std::map<std::vector<uint64_t>, uint32_t> classes;
+  // classes: distinct (label, sig_1..sig_R); program = label plane, then the
+  // thresholds in (r, l) order.  Classes are numbered in lexicographic order
+  // of their programs so consecutive classes share prefixes; cp[c] = length
+  // of the prefix class c shares with class c-1.
+  std::map<std::vector<uint16_t>, uint32_t> programs;  // program -> class
+  std::vector<uint16_t> cur;
+  std::vector<std::vector<uint16_t>> prog_of_vertex(Qn);
+  for (uint64_t v = 0; v < Qn; ++v) {
+    cur.clear();
+    cur.push_back(static_cast<uint16_t>(label_plane[lab[v]]));
+    for (uint32_t r = 0; r < R; ++r)
+      for (uint32_t l = 0; l < 16; ++l) {
+        const uint32_t c = sig_get(sig[r * Qn + v], l);
+        if (c) cur.push_back(static_cast<uint16_t>(ge_plane[(r << 16) | (l << 8) | c]));
+      }
+    programs.emplace(cur, 0u);
+    prog_of_vertex[v] = cur;
+  }
   std::vector<uint32_t> cls(Qn), prog_off{0};
   std::vector<uint16_t> prog;
-  std::vector<uint64_t> key(R + 1);
-  for (uint64_t v = 0; v < Qn; ++v) {
-    key[0] = lab[v];
-    for (uint32_t r = 0; r < R; ++r) key[r + 1] = sig[r * Qn + v];
-    auto it = classes.find(key);
-    if (it == classes.end()) {
-      const uint32_t id = static_cast<uint32_t>(classes.size());
-      it = classes.emplace(key, id).first;
-      prog.push_back(static_cast<uint16_t>(label_plane[lab[v]]));
-      for (uint32_t r = 0; r < R; ++r)
-        for (uint32_t l = 0; l < 16; ++l) {
-          const uint32_t c = sig_get(key[r + 1], l);
-          if (c) prog.push_back(static_cast<uint16_t>(ge_plane[(r << 16) | (l << 8) | c]));
-        }
-      prog_off.push_back(static_cast<uint32_t>(prog.size()));
-    }
-    cls[v] = it->second;
+  std::vector<uint8_t> cp;
+  const std::vector<uint16_t>* prev = nullptr;
+  uint32_t max_len = 0;
+  for (auto& kv : programs) {
+    kv.second = static_cast<uint32_t>(cp.size());
+    uint32_t common = 0;
+    if (prev)
+      while (common < prev->size() && common < kv.first.size() && (*prev)[common] == kv.first[common]) ++common;
+    cp.push_back(static_cast<uint8_t>(common < 255 ? common : 255));
+    prog.insert(prog.end(), kv.first.begin(), kv.first.end());
+    prog_off.push_back(static_cast<uint32_t>(prog.size()));
+    max_len = std::max<uint32_t>(max_len, static_cast<uint32_t>(kv.first.size()));
+    prev = &kv.first;
   }
+  for (uint64_t v = 0; v < Qn; ++v) cls[v] = programs[prog_of_vertex[v]];
+  std::map<std::vector<uint16_t>, uint32_t>& classes = programs;
   pp.K = static_cast<uint32_t>(spec.size());
   pp.C = static_cast<uint32_t>(classes.size());
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.spec), spec.data(), 4 * spec.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog_off), prog_off.data(), 4 * prog_off.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog), prog.data(), 2 * prog.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.cls), cls.data(), 4 * cls.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.cp), cp.data(), cp.size()));
+  pp.max_len = max_len;
   SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
   pp.R = R;
   pp.profile = q->opts.profile;
@@ -182,16 +199,20 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   p += al(b_lplanes);
   uint32_t* lbits = reinterpret_cast<uint32_t*>(p);
   int rc = launch_sig_all(q, data, R, dsig);
-  if (!rc && b_planes && cudaMemsetAsync(planes, 0, b_planes, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
-  if (!rc) rc = launch_build_planes(q, data, dsig, R, pp, planes);
   if (!rc && cudaEventRecord(ev.e[1], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
-  if (!rc) rc = launch_ne_planes(q, data, pp, planes, NE);
+  if (!rc) rc = launch_planes_ne(q, data, dsig, R, pp, planes, NE);
   if (!rc && cudaEventRecord(ev.e[2], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
   if (!rc) rc = launch_gmcr_from_ne(q, query, data, NE, pp.cls, m, true, 0);
   if (!rc && cudaEventRecord(ev.e[3], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
-  if (!rc && L && m->total) {
+  const bool literal = !rc && L && m->total;
+  if (literal) {
     // REF_PTX: graphs starting below vertex 256 keep the reference's live
-    // `visited` bitset, so they take the literal join on the bitset words it reads.
+    // `visited` bitset, so they take the literal join on the bitset words it
+    // reads.  That runs on the side stream, overlapping the fast join.
+    const cudaStream_t main_stream = q->stream;
+    if (cudaEventRecord(q->ev_fork, main_stream) != cudaSuccess || cudaStreamWaitEvent(q->side, q->ev_fork, 0) != cudaSuccess)
+      rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
+    q->stream = q->side;
     for (uint32_t r = 0; r < R && !rc; ++r)
       rc = launch_sig_planes(q, dsig + static_cast<uint64_t>(r) * N, N, Wlp, lplanes + static_cast<uint64_t>(r) * 16 * 4 * Wlp);
     if (!rc) rc = launch_fused_filter_raw(q, query->node_labels, pp.qsig_all, Qn, data->node_labels, N, lplanes, Wlp, R, lbits);
@@ -203,8 +224,12 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
     view.Wp = Wlp;
     view.bits = lbits;
     if (!rc) rc = launch_join_literal(q, query, data, &view, m, find_first, 0, L, d_total);
+    q->stream = main_stream;
   }
   if (!rc) rc = launch_join_fast_planes(q, query, data, pp, planes, m, find_first, d_total);
+  // join the side stream back before the scratch is released and the total read
+  if (cudaEventRecord(q->ev_join, q->side) != cudaSuccess || cudaStreamWaitEvent(q->stream, q->ev_join, 0) != cudaSuccess)
+    rc = rc ? rc : fail(SIGMO_ERR_CUDA, "stream join failed");
   dev_free(q, buf);
   return rc;
 }

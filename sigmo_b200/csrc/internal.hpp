@@ -37,6 +37,8 @@ struct Queue {
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
   void* pinned = nullptr;  // small pinned host buffer for scalar read-backs
+  cudaStream_t side = nullptr;  // second stream for work that overlaps the main one
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 // Per-query-batch plane program of the batched form (kernels_planes.cu).
@@ -50,6 +52,8 @@ struct PlaneProgram {
   uint32_t* prog_off = nullptr;   // [C + 1]
   uint16_t* prog = nullptr;       // plane indices of each class's program
   uint32_t* cls = nullptr;        // [query vertices] class of each vertex
+  uint8_t* cp = nullptr;          // [C] prefix shared with the previous class's program
+  uint32_t max_len = 0;           // longest program
   uint64_t* qsig_all = nullptr;   // [R][query vertices] signatures, iterations 1..R
 };
 
@@ -96,7 +100,7 @@ struct Signature {
   uint64_t* data_reach = nullptr;
   uint64_t* query_reach = nullptr;
   uint32_t reach_words = 1;  // 1 (REF_PTX) or 4 (EXACT)
-  uint32_t* data_planes = nullptr;  // bit-sliced data signatures [16][Wp] x uint4
+  uint32_t* data_planes = nullptr;  // thermometer planes of the data signatures [16*15][Wp]
   uint64_t planes_Wp = 0;
   bool planes_valid = false;
 };
@@ -138,8 +142,9 @@ int launch_sig_generate(Queue* q, const Graph* g, uint64_t* sig);
 int launch_sig_refine(Queue* q, const Graph* g, uint32_t view, uint64_t* sig, uint64_t* reach, uint32_t reach_words);
 int launch_sig_all(Queue* q, const Graph* g, uint32_t R, uint64_t* sig_all /* [R][N] */);
 int launch_sig_planes(Queue* q, const uint64_t* sig, uint64_t n, uint64_t Wp, uint32_t* planes);
+int launch_sig_thermo(Queue* q, const uint64_t* sig, uint64_t n, uint64_t Wp, uint32_t* therm);
 int launch_filter(Queue* q, const Graph* query, const Graph* data, Candidates* c);
-int launch_refine(Queue* q, const Graph* query, const Graph* data, const uint64_t* qsig, const uint32_t* planes,
+int launch_refine(Queue* q, const Graph* query, const Graph* data, const uint64_t* qsig, const uint32_t* therm,
                   Candidates* c);
 int launch_fused_filter(Queue* q, const Graph* query, const Graph* data, uint32_t R, const uint64_t* qsig_all,
                         const uint32_t* planes_all, Candidates* c);
@@ -153,9 +158,8 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
                             Gmcr* m, int find_first, uint64_t* d_total);
 int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const uint32_t* NE, const uint32_t* cls, Gmcr* m,
                         bool sync_total, uint64_t capacity_hint);
-int launch_build_planes(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
-                        uint64_t* planes);
-int launch_ne_planes(Queue* q, const Graph* data, const PlaneProgram& pp, const uint64_t* planes, uint32_t* NE);
+int launch_planes_ne(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
+                     uint64_t* planes, uint32_t* NE);
 size_t ne_planes_smem(uint32_t K, uint32_t AW);
 int launch_fused_filter_raw(Queue* q, const uint8_t* qlab, const uint64_t* qsig_all, uint64_t Qn, const uint8_t* dlab,
                             uint64_t N, const uint32_t* planes_all, uint64_t Wstride, uint32_t R, uint32_t* bits);

@@ -117,9 +117,37 @@ __global__ void k_sig_planes(const uint64_t* __restrict__ sig, uint64_t n, uint6
   }
 }
 
-// refineCandidates: C[q][w] &= dominance(sig_q, planes of word w).  Rows are
-// processed four at a time so four independent loads are in flight.
-__global__ void k_refine(const uint64_t* __restrict__ qsig, uint64_t Qn, const uint4* __restrict__ planes, uint64_t Wp,
+// Thermometer planes of the current data signatures: plane p = l*15 + (c-1)
+// (l < 16, c = 1..15) has bit i of word w set when counter l of vertex 32w+i
+// is >= c.  Warp per word, lane i = vertex 32w+i; planes are produced 32 at a
+// time, lane j keeping plane (group + j) for one store.
+__global__ void k_sig_thermo(const uint64_t* __restrict__ sig, uint64_t n, uint64_t Wp, uint32_t* __restrict__ therm) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t w = warp; w < Wp; w += nwarps) {
+    const uint64_t v = w * 32 + lane;
+    const uint64_t s = v < n ? sig[v] : 0ull;
+    for (unsigned g0 = 0; g0 < 240; g0 += 32) {
+      uint32_t mine = 0;
+#pragma unroll
+      for (unsigned j = 0; j < 32; ++j) {
+        const unsigned p = g0 + j;
+        if (p < 240) {
+          const unsigned l = p / 15, c = p % 15 + 1;
+          const uint32_t b = __ballot_sync(0xFFFFFFFFu, ((s >> (4 * l)) & 0xFu) >= c);
+          if (lane == j) mine = b;
+        }
+      }
+      if (g0 + lane < 240) therm[static_cast<uint64_t>(g0 + lane) * Wp + w] = mine;
+    }
+  }
+}
+
+// refineCandidates: C[q][w] &= AND over q's non-zero counters (l, c) of the
+// thermometer plane "counter l >= c" of word w.  Rows are processed four at a
+// time so four independent loads are in flight.
+__global__ void k_refine(const uint64_t* __restrict__ qsig, uint64_t Qn, const uint32_t* __restrict__ therm, uint64_t Wp,
                          uint64_t W, uint32_t* __restrict__ bits) {
   const uint64_t w = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
   if (w >= W) return;
@@ -132,7 +160,15 @@ __global__ void k_refine(const uint64_t* __restrict__ qsig, uint64_t Qn, const u
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (!wd[k]) continue;
-      const uint32_t m = dominance_word(qsig[q + k], planes, Wp, w, wd[k]);
+      const uint64_t qs = qsig[q + k];
+      uint64_t nz = sig_nonzero_nibbles(qs);
+      uint32_t m = wd[k];
+      while (nz) {
+        const uint32_t p = __ffsll(static_cast<long long>(nz)) - 1;  // 4 * label
+        nz &= nz - 1;
+        const uint32_t c = static_cast<uint32_t>((qs >> p) & 0xFu);
+        m &= __ldg(therm + static_cast<uint64_t>((p >> 2) * 15 + c - 1) * Wp + w);
+      }
       if (m != wd[k]) bits[(q + k) * Wp + w] = m;
     }
   }
@@ -223,14 +259,21 @@ int launch_sig_planes(Queue* q, const uint64_t* sig, uint64_t n, uint64_t Wp, ui
   return check_launch(q, "k_sig_planes");
 }
 
-int launch_refine(Queue* q, const Graph* query, const Graph* data, const uint64_t* qsig, const uint32_t* planes,
+int launch_sig_thermo(Queue* q, const uint64_t* sig, uint64_t n, uint64_t Wp, uint32_t* therm) {
+  if (!Wp) return SIGMO_OK;
+  const unsigned threads = 256;
+  k_sig_thermo<<<grid_for(Wp * 32, threads, 148u * 16u), threads, 0, q->stream>>>(sig, n, Wp, therm);
+  return check_launch(q, "k_sig_thermo");
+}
+
+int launch_refine(Queue* q, const Graph* query, const Graph* data, const uint64_t* qsig, const uint32_t* therm,
                   Candidates* c) {
   (void)query;
   (void)data;
   if (!c->rows || !c->W) return SIGMO_OK;
   dim3 grid(grid_for(c->W, kWordsPerBlock), static_cast<unsigned>((c->rows + kRowsPerBlock - 1) / kRowsPerBlock));
   if (grid.y > 65535u) return fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", (unsigned long long)c->rows);
-  k_refine<<<grid, kWordsPerBlock, 0, q->stream>>>(qsig, c->rows, reinterpret_cast<const uint4*>(planes), c->Wp, c->W, c->bits);
+  k_refine<<<grid, kWordsPerBlock, 0, q->stream>>>(qsig, c->rows, therm, c->Wp, c->W, c->bits);
   return check_launch(q, "k_refine");
 }
 

@@ -76,6 +76,49 @@ struct Frame {
   uint32_t idx;
 };
 
+// Per-pair cache of the range-masked candidate words of every query vertex
+// (a data graph of <= 64 vertices spans at most 3 bitset words), so the DFS's
+// repeated getCandidatesCount / getCandidateAt read registers/L1 instead of
+// the bitset.  Values are exactly those of candidates.hpp:86-162.
+struct PairCands {
+  uint32_t w[kMaxQueryNodes][3];
+  uint32_t cnt[kMaxQueryNodes];
+  uint32_t i0, nw;
+  __device__ __forceinline__ void load(const uint32_t* __restrict__ bits, uint64_t Wp, uint32_t qoff, uint32_t n, uint32_t s,
+                                       uint32_t e, int prof) {
+    i0 = s >> 5;
+    nw = ((e + 31u) >> 5) - i0;
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t* row = bits + static_cast<uint64_t>(qoff + j) * Wp;
+      uint32_t c = 0;
+      for (uint32_t k = 0; k < 3; ++k) {
+        const uint32_t v = k < nw ? (row[i0 + k] & range_mask(i0 + k, s, e, prof)) : 0u;
+        w[j][k] = v;
+        c += __popc(v);
+      }
+      cnt[j] = c;
+    }
+  }
+  __device__ __forceinline__ uint32_t at(uint32_t j, uint32_t idx) const {
+    uint32_t c = 0;
+    for (uint32_t k = 0; k < nw; ++k) {
+      uint32_t blk = w[j][k];
+      const uint32_t bc = __popc(blk);
+      if (c + bc > idx) {
+        while (blk) {
+          const uint32_t t = __ffs(blk) - 1;
+          if (c == idx) return ((i0 + k) << 5) + t;
+          blk &= blk - 1;
+          ++c;
+        }
+      } else {
+        c += bc;
+      }
+    }
+    return 0xFFFFFFFFu;
+  }
+};
+
 template <bool EXACT>
 __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, int prof,
                                const uint32_t* __restrict__ qgoff, const uint64_t* __restrict__ qadj,
@@ -86,8 +129,12 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
                                unsigned long long* __restrict__ d_total) {
   const uint32_t wg = blockDim.x, lid = threadIdx.x;
   uint64_t my_total = 0;
+  PairCands pc;
+  uint64_t rowc[kMaxQueryNodes];   // adjacency row of mapping[i] (graphs <= 64 vertices)
+  uint64_t vmask[kMaxQueryNodes];  // candidates passing isValidMapping at depth d (graphs <= 64 vertices)
   for (uint32_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
     const uint32_t s = dgoff[g], e = dgoff[g + 1], ng = e - s;
+    const bool small = ng <= 64u;
     const uint32_t seg0 = offsets[g], seglen = offsets[g + 1] - seg0;
     uint32_t mapping[kMaxQueryNodes + 1];
 #pragma unroll 1
@@ -95,6 +142,36 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
     for (uint32_t it = lid; it < seglen; it += wg) {
       const uint32_t qg = indices[seg0 + it];
       const uint32_t qoff = qgoff[qg], n = qgoff[qg + 1] - qoff;
+      if (small) pc.load(bits, Wp, qoff, n, s, e, prof);
+      auto count_of = [&](uint32_t qn) -> uint32_t {
+        return small ? pc.cnt[qn] : cand_count(bits + static_cast<uint64_t>(qoff + qn) * Wp, s, e, prof);
+      };
+      auto cand_of = [&](uint32_t qn, uint32_t idx) -> uint32_t {
+        return small ? pc.at(qn, idx) : cand_at(bits + static_cast<uint64_t>(qoff + qn) * Wp, idx, s, e, prof);
+      };
+      // isValidMapping (isomorphism.hpp:150-168).  Its result depends only on
+      // mapping[0..qn-1], which stay fixed while the frame at depth qn runs, so
+      // for graphs of <= 64 vertices it is evaluated once per push as the bit
+      // set vmask[qn] and each candidate is then one bit test.
+      auto valid = [&](uint32_t qn, uint32_t cand) -> bool {
+        if (small) return (vmask[qn] >> (cand - s)) & 1ull;
+        const uint64_t qrow_bit = 1ull << qn;
+        for (uint32_t i = 0; i < qn; ++i) {
+          const bool qa = (qadj[qoff + i] & qrow_bit) != 0;
+          if (qa != data_neighbor(mapping[i], cand, s, ng, dadj, dAW, droff, dcol)) return false;
+        }
+        return true;
+      };
+      // vmask[d] from rowc[0..d-1]: local t is valid iff for every i < d,
+      // (d in query row i) == (t in data row of mapping[i]).
+      auto push_mask = [&](uint32_t d) {
+        if (!small || d >= n) return;
+        uint64_t vm = ~0ull;
+        const uint64_t qbit = 1ull << d;
+        for (uint32_t i = 0; i < d; ++i) vm &= ((qadj[qoff + i] & qbit) ? rowc[i] : ~rowc[i]);
+        vmask[d] = vm;
+      };
+      if (small) vmask[0] = ~0ull;
       uint64_t found = 0;
       Frame stack[kMaxQueryNodes + 2];
       uint32_t top = 0;
@@ -110,25 +187,21 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
             if (find_first) break;
             continue;
           }
-          const uint32_t* row = bits + static_cast<uint64_t>(qoff + qn) * Wp;
-          if (fr.idx >= cand_count(row, s, e, prof)) {
+          if (fr.idx >= count_of(qn)) {
             --top;
             visited &= ~refbit(mapping[qn], s);
             if (top == 1) visited = 0;
             continue;
           }
-          const uint32_t cand = cand_at(row, fr.idx, s, e, prof);
+          const uint32_t cand = cand_of(qn, fr.idx);
           stack[top - 1].idx++;
           if (visited & refbit(cand, s)) continue;
-          bool ok = true;
-          for (uint32_t i = 0; i < qn && ok; ++i) {
-            const bool qa = (qadj[qoff + i] >> qn) & 1ull;
-            ok = qa == data_neighbor(mapping[i], cand, s, ng, dadj, dAW, droff, dcol);
-          }
-          if (ok) {
+          if (valid(qn, cand)) {
             mapping[qn] = cand;
+            if (small) rowc[qn] = dadj[static_cast<uint64_t>(cand) * dAW];
             visited |= refbit(cand, s);
             stack[top++] = {qn + 1, 0u};
+            push_mask(qn + 1);
           }
         }
       } else {
@@ -151,25 +224,21 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
             used[t >> 6] &= ~(1ull << (t & 63u));
             placed[qn] = 0xFFFFFFFFu;
           }
-          const uint32_t* row = bits + static_cast<uint64_t>(qoff + qn) * Wp;
-          if (fr.idx >= cand_count(row, s, e, prof)) {
+          if (fr.idx >= count_of(qn)) {
             --top;
             continue;
           }
-          const uint32_t cand = cand_at(row, fr.idx, s, e, prof);
+          const uint32_t cand = cand_of(qn, fr.idx);
           stack[top - 1].idx++;
           const uint32_t t = cand - s;
           if ((used[t >> 6] >> (t & 63u)) & 1ull) continue;
-          bool ok = true;
-          for (uint32_t i = 0; i < qn && ok; ++i) {
-            const bool qa = (qadj[qoff + i] >> qn) & 1ull;
-            ok = qa == data_neighbor(mapping[i], cand, s, ng, dadj, dAW, droff, dcol);
-          }
-          if (ok) {
+          if (valid(qn, cand)) {
             mapping[qn] = cand;
+            if (small) rowc[qn] = dadj[static_cast<uint64_t>(cand) * dAW];
             placed[qn] = cand;
             used[t >> 6] |= 1ull << (t & 63u);
             stack[top++] = {qn + 1, 0u};
+            push_mask(qn + 1);
           }
         }
       }
@@ -230,6 +299,11 @@ __device__ __forceinline__ void mask_from_planes(const uint64_t* __restrict__ pl
   }
 }
 
+// Persistent join over GMCR slots.  Each lane runs its own DFS as a flat
+// state machine — one loop iteration expands one node — and pulls a new pair
+// when its current one is finished, so lanes of a warp stay busy regardless of
+// how uneven the pairs are.  Lanes needing work take kChunk consecutive slots
+// each with one warp-aggregated atomic.
 template <int AW, bool EXACT, bool FROM_PLANES>
 __global__ void __launch_bounds__(128) k_join_fast(
     const uint32_t* __restrict__ bits, uint64_t Wp, const uint64_t* __restrict__ planes, uint32_t K,
@@ -238,94 +312,253 @@ __global__ void __launch_bounds__(128) k_join_fast(
     const uint8_t* __restrict__ qorder, const uint64_t* __restrict__ qsel, const uint64_t* __restrict__ qsel_id,
     const uint8_t* __restrict__ qsym, const uint32_t* __restrict__ dgoff, const uint64_t* __restrict__ dadj,
     const uint8_t* __restrict__ dsym, const uint32_t* __restrict__ indices, const uint32_t* __restrict__ pair_graph,
-    uint64_t total, uint32_t skip_below, int find_first, unsigned long long* __restrict__ cursor,
-    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total) {
-  constexpr uint32_t kChunk = 8;  // slots per lane per warp grab
+    const uint32_t* __restrict__ list, const unsigned long long* __restrict__ list_len, uint64_t total_slots,
+    uint32_t skip_below, int find_first, unsigned long long* __restrict__ cursor, uint64_t* __restrict__ counts,
+    unsigned long long* __restrict__ d_total) {
+  constexpr uint32_t kChunk = 8;
+  const uint64_t total = list ? *list_len : total_slots;  // entries to walk (list or all slots)
   const unsigned lane = threadIdx.x & 31u;
   uint64_t my_total = 0;
   uint64_t M[kMaxQueryNodes][AW];     // candidates of each level (graph-local)
   uint64_t cand[kMaxQueryNodes][AW];  // untried candidates of each level
   uint64_t rows[kMaxQueryNodes][AW];  // adjacency row of each level's pick
   uint32_t pick[kMaxQueryNodes];
+  uint64_t next = 0, end = 0;  // this lane's claimed slot range
+  uint64_t slot = 0;
+  uint64_t cnt = 0;
+  uint32_t n = 0, s = 0;
+  const uint64_t* selp = nullptr;
+  int k = -1;  // DFS level; -1 = no pair in progress
+  bool have = false;
   for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(cursor, 32ull * kChunk);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= total) break;
-    for (uint32_t c = 0; c < kChunk; ++c) {
-      const uint64_t slot = base + c * 32ull + lane;
-      if (slot >= total) break;
+    if (k < 0) {
+      if (have) {
+        if (find_first && cnt) cnt = 1;
+        counts[slot] = cnt;
+        my_total += cnt;
+        have = false;
+      }
+      // claim the next slot of a pair this kernel handles
+      bool done = false;
+      for (;;) {
+        if (next >= end) {
+          const unsigned am = __activemask();
+          const unsigned leader = __ffs(am) - 1;
+          const unsigned rank = __popc(am & ((1u << lane) - 1u));
+          unsigned long long base = 0;
+          if (lane == leader) base = atomicAdd(cursor, static_cast<unsigned long long>(__popc(am)) * kChunk);
+          base = __shfl_sync(am, base, leader);
+          next = base + static_cast<uint64_t>(rank) * kChunk;
+          end = next + kChunk < total ? next + kChunk : total;
+          if (next >= total) {
+            done = true;
+            break;
+          }
+        }
+        slot = list ? list[next] : next;
+        ++next;
+        if (pair_graph[slot] >= skip_below) break;
+      }
+      if (done) break;
       const uint32_t g = pair_graph[slot];
-      if (g < skip_below) continue;
       const uint32_t qg = indices[slot];
-      const uint32_t qoff = qgoff[qg], n = qgoff[qg + 1] - qoff;
-      const uint32_t s = dgoff[g], e = dgoff[g + 1];
+      const uint32_t qoff = qgoff[qg];
+      n = qgoff[qg + 1] - qoff;
+      s = dgoff[g];
+      const uint32_t e = dgoff[g + 1];
       const bool ident = !(qsym[qg] && dsym[g]);
-      const uint64_t* selp = (ident ? qsel_id : qsel) + qoff;
-      for (uint32_t k = 0; k < n; ++k) {
-        const uint32_t v = ident ? k : qorder[qoff + k];
-        if (FROM_PLANES) mask_from_planes<AW>(planes, K, g, cls[qoff + v], prog_off, prog, M[k]);
-        else extract_local<AW>(bits + static_cast<uint64_t>(qoff + v) * Wp, s, e, prof, M[k]);
+      selp = (ident ? qsel_id : qsel) + qoff;
+      for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t v = ident ? j : qorder[qoff + j];
+        if (FROM_PLANES) mask_from_planes<AW>(planes, K, g, cls[qoff + v], prog_off, prog, M[j]);
+        else extract_local<AW>(bits + static_cast<uint64_t>(qoff + v) * Wp, s, e, prof, M[j]);
       }
 #pragma unroll
       for (int w = 0; w < AW; ++w) cand[0][w] = M[0][w];
-      uint64_t cnt = 0;
-      int k = 0;
-      while (k >= 0) {
-        bool empty = true;
-#pragma unroll
-        for (int w = 0; w < AW; ++w) empty &= cand[k][w] == 0;
-        if (empty) {
-          --k;
-          continue;
-        }
-        uint32_t t = 0;
-#pragma unroll
-        for (int w = AW - 1; w >= 0; --w)
-          if (cand[k][w]) t = 64u * w + (__ffsll(static_cast<long long>(cand[k][w])) - 1);
-        cand[k][t >> 6] &= cand[k][t >> 6] - 1;
-        pick[k] = t;
-        const uint64_t* r = dadj + static_cast<uint64_t>(s + t) * AW;
-#pragma unroll
-        for (int w = 0; w < AW; ++w) rows[k][w] = r[w];
-        const uint64_t sl = selp[k + 1];
-        uint64_t nx[AW], excl[AW];
-#pragma unroll
-        for (int w = 0; w < AW; ++w) {
-          nx[w] = M[k + 1][w];
-          excl[w] = 0;
-        }
-        for (int i = 0; i <= k; ++i) {
-          const bool adjq = (sl >> i) & 1ull;
-#pragma unroll
-          for (int w = 0; w < AW; ++w) nx[w] &= adjq ? rows[i][w] : ~rows[i][w];
-          if (EXACT) {
-#pragma unroll
-            for (int w = 0; w < AW; ++w)
-              if ((pick[i] >> 6) == static_cast<uint32_t>(w)) excl[w] |= 1ull << (pick[i] & 63u);
-          }
-        }
-        if (EXACT) {
-#pragma unroll
-          for (int w = 0; w < AW; ++w) nx[w] &= ~excl[w];
-        }
-        if (static_cast<uint32_t>(k + 1) == n - 1) {
-          uint32_t pc = 0;
-#pragma unroll
-          for (int w = 0; w < AW; ++w) pc += __popcll(nx[w]);
-          cnt += pc;
-          if (find_first && cnt) break;
-          continue;
-        }
-        ++k;
-#pragma unroll
-        for (int w = 0; w < AW; ++w) cand[k][w] = nx[w];
-      }
-      if (find_first && cnt) cnt = 1;
-      counts[slot] = cnt;
-      my_total += cnt;
+      cnt = 0;
+      k = 0;
+      have = true;
+      continue;
     }
+    // one DFS node at level k
+    bool empty = true;
+#pragma unroll
+    for (int w = 0; w < AW; ++w) empty &= cand[k][w] == 0;
+    if (empty) {
+      --k;
+      continue;
+    }
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = AW - 1; w >= 0; --w)
+      if (cand[k][w]) t = 64u * w + (__ffsll(static_cast<long long>(cand[k][w])) - 1);
+    cand[k][t >> 6] &= cand[k][t >> 6] - 1;
+    pick[k] = t;
+    const uint64_t* r = dadj + static_cast<uint64_t>(s + t) * AW;
+#pragma unroll
+    for (int w = 0; w < AW; ++w) rows[k][w] = r[w];
+    const uint64_t sl = selp[k + 1];
+    uint64_t nx[AW], excl[AW];
+#pragma unroll
+    for (int w = 0; w < AW; ++w) {
+      nx[w] = M[k + 1][w];
+      excl[w] = 0;
+    }
+    for (int i = 0; i <= k; ++i) {
+      const uint64_t keep_set = 0ull - ((sl >> i) & 1ull);  // all ones when adjacent in the query
+#pragma unroll
+      for (int w = 0; w < AW; ++w) nx[w] &= ~(rows[i][w] ^ keep_set) ;
+      if (EXACT) {
+#pragma unroll
+        for (int w = 0; w < AW; ++w)
+          if ((pick[i] >> 6) == static_cast<uint32_t>(w)) excl[w] |= 1ull << (pick[i] & 63u);
+      }
+    }
+    if (EXACT) {
+#pragma unroll
+      for (int w = 0; w < AW; ++w) nx[w] &= ~excl[w];
+    }
+    if (static_cast<uint32_t>(k + 1) == n - 1) {
+      uint32_t pc = 0;
+#pragma unroll
+      for (int w = 0; w < AW; ++w) pc += __popcll(nx[w]);
+      cnt += pc;
+      if (find_first && cnt) k = -1;
+      continue;
+    }
+    ++k;
+#pragma unroll
+    for (int w = 0; w < AW; ++w) cand[k][w] = nx[w];
   }
+  for (int o = 16; o; o >>= 1) my_total += __shfl_xor_sync(0xFFFFFFFFu, my_total, o);
+  if (lane == 0 && my_total) atomicAdd(d_total, static_cast<unsigned long long>(my_total));
+}
+
+// Two-phase join for pairs whose query has <= kPhaseLevels vertices.
+// Phase A (k_pair_masks): per slot of a chunk and per level j, the candidate
+// set of the query vertex placed at level j = AND of its class's plane program
+// for the slot's data graph, stored [level][slot-in-chunk] (coalesced).
+// Phase B (k_join_masks): the DFS as a flat per-lane state machine whose pair
+// setup is just the load of those masks, with the per-level state in shared
+// memory ([level][thread]).  Trying a candidate t at level k is O(1):
+// next = base[k+1] & (row(t) or ~row(t)) [& ~used]; base[k+2] is computed
+// once per descent.
+constexpr uint32_t kPhaseLevels = 16;
+constexpr uint32_t kPhaseThreads = 256;
+
+__global__ void __launch_bounds__(256) k_pair_masks(
+    const uint64_t* __restrict__ planes, uint32_t K, const uint32_t* __restrict__ prog_off, const uint16_t* __restrict__ prog,
+    const uint32_t* __restrict__ cls, const uint32_t* __restrict__ qgoff, const uint8_t* __restrict__ qorder,
+    const uint8_t* __restrict__ qsym, const uint32_t* __restrict__ dgoff, const uint8_t* __restrict__ dsym,
+    const uint32_t* __restrict__ indices, const uint32_t* __restrict__ pair_graph, uint64_t slot0, uint64_t count,
+    uint64_t* __restrict__ masks, uint4* __restrict__ rec, uint32_t skip_below, uint32_t* __restrict__ overflow,
+    unsigned long long* __restrict__ overflow_len) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count * kPhaseLevels; i += stride) {
+    const uint64_t local = i % count;  // slot within the chunk (fastest), then level
+    const uint32_t j = static_cast<uint32_t>(i / count);
+    const uint64_t slot = slot0 + local;
+    const uint32_t qg = indices[slot];
+    const uint32_t qoff = qgoff[qg], n = qgoff[qg + 1] - qoff;
+    if (j >= n) continue;
+    const uint32_t g = pair_graph[slot];
+    const bool ident = !(qsym[qg] && dsym[g]);
+    if (j == 0) {  // the pair's setup record: first data vertex, query size, query offset, order
+      rec[local] = make_uint4(dgoff[g], n | (ident ? 0x100u : 0u), qoff, g);
+      if (n > kPhaseLevels && g >= skip_below) overflow[atomicAdd(overflow_len, 1ull)] = static_cast<uint32_t>(slot);
+    }
+    if (n > kPhaseLevels) continue;
+    const uint32_t c = cls[qoff + (ident ? j : qorder[qoff + j])];
+    const uint64_t* base = planes + static_cast<uint64_t>(g >> 5) * K * 32 + (g & 31u);
+    uint64_t m = ~0ull;
+    const uint32_t e1 = prog_off[c + 1];
+    for (uint32_t e = prog_off[c]; e < e1; ++e) m &= base[static_cast<uint64_t>(prog[e]) * 32];
+    masks[static_cast<uint64_t>(j) * count + local] = m;
+  }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
+    const uint64_t* __restrict__ masks, const uint4* __restrict__ rec, uint64_t slot0, uint64_t count,
+    const uint64_t* __restrict__ qsel, const uint64_t* __restrict__ qsel_id, const uint64_t* __restrict__ dadj,
+    uint32_t skip_below, int find_first, unsigned long long* __restrict__ cursor, uint64_t* __restrict__ counts,
+    unsigned long long* __restrict__ d_total) {
+  constexpr uint32_t kChunk = 4;
+  extern __shared__ uint64_t sm[];
+  const unsigned tid = threadIdx.x, lane = tid & 31u;
+  uint64_t* cand = sm;
+  uint64_t* base = sm + kPhaseLevels * kPhaseThreads;
+  uint8_t* pk = reinterpret_cast<uint8_t*>(sm + 2 * kPhaseLevels * kPhaseThreads);
+#define AT(arr, lvl) arr[(lvl) * kPhaseThreads + tid]
+  uint64_t my_total = 0;
+  uint64_t next = 0, end = 0, local = 0, cnt = 0;
+  uint32_t n = 0, s = 0;
+  const uint64_t* selp = nullptr;
+  uint64_t used = 0;
+  int k = -1;
+  bool have = false;
+  for (;;) {
+    if (k < 0) {
+      if (have) {
+        if (find_first && cnt) cnt = 1;
+        counts[slot0 + local] = cnt;
+        my_total += cnt;
+        have = false;
+      }
+      if (next >= end) {
+        const unsigned am = __activemask();
+        const unsigned leader = __ffs(am) - 1;
+        const unsigned rank = __popc(am & ((1u << lane) - 1u));
+        unsigned long long b = 0;
+        if (lane == leader) b = atomicAdd(cursor, static_cast<unsigned long long>(__popc(am)) * kChunk);
+        b = __shfl_sync(am, b, leader);
+        next = b + static_cast<uint64_t>(rank) * kChunk;
+        end = next + kChunk < count ? next + kChunk : count;
+        if (next >= count) break;
+      }
+      local = next++;
+      const uint4 r = rec[local];  // first data vertex, query size | order flag, query offset, data graph
+      if (r.w < skip_below) continue;
+      n = r.y & 0xFFu;
+      if (n > kPhaseLevels) continue;  // in the overflow list (generic kernel)
+      s = r.x;
+      selp = ((r.y & 0x100u) ? qsel_id : qsel) + r.z;
+      AT(cand, 0) = masks[local];
+      AT(base, 1) = masks[count + local];
+      used = 0;
+      cnt = 0;
+      k = 0;
+      have = true;
+      continue;
+    }
+    const uint64_t ck = AT(cand, k);
+    if (!ck) {
+      --k;
+      if (EXACT && k >= 0) used &= ~(1ull << AT(pk, k));
+      continue;
+    }
+    const uint32_t t = __ffsll(static_cast<long long>(ck)) - 1;
+    AT(cand, k) = ck & (ck - 1);
+    const uint64_t rw = dadj[s + t];
+    const uint64_t keep = 0ull - ((selp[k + 1] >> k) & 1ull);
+    uint64_t nx = AT(base, k + 1) & ~(rw ^ keep);
+    if (EXACT) nx &= ~(used | (1ull << t));
+    if (static_cast<uint32_t>(k + 1) == n - 1) {
+      cnt += __popcll(nx);
+      if (find_first && cnt) k = -1;
+      continue;
+    }
+    if (!nx) continue;
+    AT(pk, k) = static_cast<uint8_t>(t);
+    if (EXACT) used |= 1ull << t;
+    AT(cand, k + 1) = nx;
+    const uint64_t sl2 = selp[k + 2];
+    uint64_t b2 = masks[static_cast<uint64_t>(k + 2) * count + local] & ~(rw ^ (0ull - ((sl2 >> k) & 1ull)));
+    for (int i = 0; i < k; ++i) b2 &= ~(dadj[s + AT(pk, i)] ^ (0ull - ((sl2 >> i) & 1ull)));
+    AT(base, k + 2) = b2;
+    ++k;
+  }
+#undef AT
   for (int o = 16; o; o >>= 1) my_total += __shfl_xor_sync(0xFFFFFFFFu, my_total, o);
   if (lane == 0 && my_total) atomicAdd(d_total, static_cast<unsigned long long>(my_total));
 }
@@ -378,8 +611,8 @@ int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Cand
   k_join_fast<AWV, EX, false><<<grid, block, 0, q->stream>>>(c->bits, c->Wp, nullptr, 0, nullptr, nullptr, nullptr,         \
                                                        q->opts.profile, query->graph_offsets, query->qorder,             \
                                                        query->qsel, query->qsel_id, query->sym, data->graph_offsets,     \
-                                                       data->adj, data->sym, m->indices, m->pair_graph, m->total, skip,  \
-                                                       find_first, cursor, m->counts, tot)
+                                                       data->adj, data->sym, m->indices, m->pair_graph, nullptr, nullptr, \
+                                                       m->total, skip, find_first, cursor, m->counts, tot)
   switch (data->adj_words) {
     case 1: if (exact) SIGMO_JOIN_FAST(1, true); else SIGMO_JOIN_FAST(1, false); break;
     case 2: if (exact) SIGMO_JOIN_FAST(2, true); else SIGMO_JOIN_FAST(2, false); break;
@@ -396,28 +629,81 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
     return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
   const bool exact = q->opts.profile == kProfileExact;
   SIGMO_TRY(launch_query_order(const_cast<Graph*>(query)));
-  void* cur = nullptr;
-  SIGMO_TRY(dev_alloc(q, &cur, 256));
-  auto* cursor = static_cast<unsigned long long*>(cur);
-  SIGMO_CUDA_TRY(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), q->stream));
   const uint32_t skip = exact ? 0u : data->low_offset_graphs;
-  const unsigned block = 128;
-  const unsigned grid = grid_for((m->total + 31) / 32 * 32, block, 148u * 16u);
+  void* buf = nullptr;
+  SIGMO_TRY(dev_alloc(q, &buf, 256 + 4ull * m->total));
+  auto* ctr = static_cast<unsigned long long*>(buf);  // [0] tile cursor, [1] generic cursor, [2] overflow length
+  uint32_t* overflow = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + 256);
+  SIGMO_CUDA_TRY(cudaMemsetAsync(ctr, 0, 256, q->stream));
   auto* tot = reinterpret_cast<unsigned long long*>(d_total);
+  // two-phase route for data graphs of <= 64 vertices, in chunks of slots
+  const bool tiles = data->adj_words == 1;
+  int rc = SIGMO_OK;
+  if (tiles) {
+    const uint64_t chunk = std::min<uint64_t>(m->total, 8ull << 20);
+    void* mbuf = nullptr;
+    rc = dev_alloc(q, &mbuf, 8ull * kPhaseLevels * chunk + 16ull * chunk);
+    const size_t smem = static_cast<size_t>(kPhaseLevels) * kPhaseThreads * (2 * 8 + 1);
+    cudaError_t e = cudaSuccess;
+    if (!rc) {
+      e = exact ? cudaFuncSetAttribute(k_join_masks<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem))
+                : cudaFuncSetAttribute(k_join_masks<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "k_join_masks shared-memory setup failed: %s", cudaGetErrorString(e));
+    }
+    for (uint64_t slot0 = 0; slot0 < m->total && !rc; slot0 += chunk) {
+      const uint64_t cnt = std::min<uint64_t>(chunk, m->total - slot0);
+      auto* masks = static_cast<uint64_t*>(mbuf);
+      auto* recs = reinterpret_cast<uint4*>(masks + kPhaseLevels * chunk);
+      k_pair_masks<<<grid_for(cnt * kPhaseLevels, 256, 148u * 32u), 256, 0, q->stream>>>(
+          planes, pp.K, pp.prog_off, pp.prog, pp.cls, query->graph_offsets, query->qorder, query->sym, data->graph_offsets,
+          data->sym, m->indices, m->pair_graph, slot0, cnt, masks, recs, skip, overflow, ctr + 2);
+      rc = check_launch(q, "k_pair_masks");
+      if (!rc && slot0 + chunk >= m->total && cudaEventRecord(q->ev_fork, q->stream) != cudaSuccess)
+        rc = fail(SIGMO_ERR_CUDA, "event record failed");
+      if (!rc) {
+        SIGMO_CUDA_TRY(cudaMemsetAsync(ctr, 0, 8, q->stream));
+        const unsigned grid = 148u * 3u;
+        if (exact)
+          k_join_masks<true><<<grid, kPhaseThreads, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id,
+                                                                         data->adj, skip, find_first, ctr, m->counts, tot);
+        else
+          k_join_masks<false><<<grid, kPhaseThreads, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id,
+                                                                          data->adj, skip, find_first, ctr, m->counts, tot);
+        rc = check_launch(q, "k_join_masks");
+      }
+    }
+    dev_free(q, mbuf);
+  }
+  const cudaStream_t main_stream = q->stream;
+  if (!rc && tiles) {
+    // the overflow list is complete after the last Phase A: its pairs run on
+    // the side stream, overlapping Phase B (the caller joins the side stream)
+    if (cudaStreamWaitEvent(q->side, q->ev_fork, 0) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
+    q->stream = q->side;
+  }
+  if (!rc) {
+    // the overflow list (two-phase route) or every slot (otherwise) through the generic kernel
+    const unsigned block = 128;
+    const unsigned grid = 148u * 8u;
+    const uint32_t* list = tiles ? overflow : nullptr;
+    const unsigned long long* list_len = tiles ? ctr + 2 : nullptr;
 #define SIGMO_JOIN_PLANES(AWV, EX)                                                                                      \
   k_join_fast<AWV, EX, true><<<grid, block, 0, q->stream>>>(nullptr, 0, planes, pp.K, pp.prog_off, pp.prog, pp.cls,      \
                                                             q->opts.profile, query->graph_offsets, query->qorder,        \
                                                             query->qsel, query->qsel_id, query->sym, data->graph_offsets, \
-                                                            data->adj, data->sym, m->indices, m->pair_graph, m->total,   \
-                                                            skip, find_first, cursor, m->counts, tot)
-  switch (data->adj_words) {
-    case 1: if (exact) SIGMO_JOIN_PLANES(1, true); else SIGMO_JOIN_PLANES(1, false); break;
-    case 2: if (exact) SIGMO_JOIN_PLANES(2, true); else SIGMO_JOIN_PLANES(2, false); break;
-    default: if (exact) SIGMO_JOIN_PLANES(4, true); else SIGMO_JOIN_PLANES(4, false); break;
-  }
+                                                            data->adj, data->sym, m->indices, m->pair_graph, list,       \
+                                                            list_len, m->total, skip, find_first, ctr + 1, m->counts, tot)
+    switch (data->adj_words) {
+      case 1: if (exact) SIGMO_JOIN_PLANES(1, true); else SIGMO_JOIN_PLANES(1, false); break;
+      case 2: if (exact) SIGMO_JOIN_PLANES(2, true); else SIGMO_JOIN_PLANES(2, false); break;
+      default: if (exact) SIGMO_JOIN_PLANES(4, true); else SIGMO_JOIN_PLANES(4, false); break;
+    }
 #undef SIGMO_JOIN_PLANES
-  int rc = check_launch(q, "k_join_fast<planes>");
-  dev_free(q, cur);
+    rc = check_launch(q, "k_join_fast<planes>");
+  }
+  q->stream = main_stream;
+  if (tiles && cudaEventRecord(q->ev_join, q->side) == cudaSuccess) cudaStreamWaitEvent(q->stream, q->ev_join, 0);
+  dev_free(q, buf);
   return rc;
 }
 
