@@ -204,6 +204,29 @@ SIGMO_API int sigmo_gmcr_total(sigmo_gmcr_t m, uint64_t* total);
 SIGMO_API int sigmo_gmcr_download(sigmo_gmcr_t m, uint32_t* offsets, uint64_t offsets_len, uint32_t* indices,
                         uint64_t indices_len);
 
+/* GMCR into caller-owned device buffers, with no device allocation at all.
+ * This entry point has no counterpart in the reference.  It is for callers
+ * that cannot allocate device memory while it runs: code working inside a
+ * fixed device-memory arena owned by another allocator, real-time services
+ * that forbid cudaMalloc/cudaFree on their request path after start-up, and
+ * callers that cannot afford the implicit synchronisation an allocation may
+ * bring.  Results equal sigmo_gmcr_generate's: d_offsets receives
+ * data_graph_offsets [num_data_graphs + 1], d_indices the first *total
+ * query_graph_indices (capacity = d_indices length in entries), *total the
+ * number of admitted pairs (also returned with SIGMO_ERR_INVALID when it
+ * exceeds capacity).  Intermediates live in one 32 MiB device array that is
+ * part of the library (every GPU that loads it holds the array until exit):
+ * batches needing more (query vertices x ceil(data graphs / 32) x 4 bytes plus
+ * query graphs x the same, plus 4 bytes per data graph) are rejected with
+ * SIGMO_ERR_DOMAIN.  The first call on a device resolves the array's device
+ * address; make that first call before any stream capture.  Every call shares
+ * the array, so calls whose work overlaps on the GPU (several queues or
+ * threads at once) race; the array keeps the last call's contents.  The call
+ * synchronises its queue once (to read the total); its last kernel may still
+ * be running on return — wait on the queue before reading d_indices. */
+SIGMO_API int sigmo_gmcr_generate_noalloc(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c,
+                                          uint32_t* d_offsets, uint32_t* d_indices, uint64_t capacity, uint64_t* total);
+
 /* ---- join (isomorphism::join::joinCandidates, isomorphism.hpp:270-381) ---- */
 /* Adds the number of matches to *num_matches (host, caller-zeroed, like the
  * reference's USM counter, sigmo.cpp:145-146).  find_first: at most one match

@@ -91,6 +91,7 @@ SIGNATURES = {
     "sigmo_gmcr_generate": (_i, [_vp, _vp, _vp, _vp]),
     "sigmo_gmcr_total": (_i, [_vp, _P(_u64)]),
     "sigmo_gmcr_download": (_i, [_vp, _vp, _u64, _vp, _u64]),
+    "sigmo_gmcr_generate_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _u64, _P(_u64)]),
     "sigmo_join_candidates": (_i, [_vp, _vp, _vp, _vp, _vp, _P(_u64), _i, _vp]),
     "sigmo_match_batched": (_i, [_vp, _vp, _vp, _u32, _i, _u32, _vp, _vp, _P(MatchResultC)]),
     "sigmo_match_download_counts": (_i, [_vp, _vp, _u64]),

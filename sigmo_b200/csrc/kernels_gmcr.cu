@@ -14,6 +14,8 @@
 
 #include <cub/device/device_scan.cuh>
 
+#include <mutex>
+
 #include "internal.hpp"
 
 namespace sigmo_b200 {
@@ -102,7 +104,7 @@ __global__ void k_gmcr_fill(const uint32_t* __restrict__ admit, uint32_t GW, uin
       if ((a >> lane) & 1u) {
         if (cur < capacity) {
           indices[cur] = q;
-          pair_graph[cur] = g;
+          if (pair_graph) pair_graph[cur] = g;
         }
         ++cur;
       }
@@ -205,4 +207,101 @@ int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidate
   return rc;
 }
 
+// ---- GMCR without device allocation ----------------------------------------
+// Some callers cannot allocate device memory while this step runs: code that
+// works inside a fixed device-memory arena owned by another allocator (a host
+// framework's caching allocator that has reserved the free memory), real-time
+// services that forbid cudaMalloc/cudaFree on their request path after
+// start-up, and callers that cannot afford the implicit synchronisation an
+// allocation or free may bring.  sigmo_gmcr_generate_noalloc computes the same
+// GMCR as sigmo_gmcr_generate with every intermediate (non-empty matrix,
+// admission words, per-graph counts, scan temporary storage) in one
+// file-scope device array and the results in buffers the caller owns.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB; every GPU that loads the library holds it until exit
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[128] = {};  // device address of g_noalloc_scratch on each device
+
+// Device address of the scratch array on `device`, which must be current.
+// In host code the array's name is only a host-side stand-in, so the address
+// is resolved once per device with cudaGetSymbolAddress (the first call on a
+// device does this set-up).
+int noalloc_scratch(int device, void** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (device < 0 || device >= 128) return fail(SIGMO_ERR_NO_DEVICE, "device %d out of range", device);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(SIGMO_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s", cudaGetErrorString(e));
+    g_noalloc_addr[device] = p;
+  }
+  *out = g_noalloc_addr[device];
+  return SIGMO_OK;
+}
+
+}  // namespace
 }  // namespace sigmo_b200
+
+extern "C" int sigmo_gmcr_generate_noalloc(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c,
+                                           uint32_t* d_offsets, uint32_t* d_indices, uint64_t capacity, uint64_t* total) {
+  using namespace sigmo_b200;
+  if (!q || !query || !data || !c || !d_offsets || !total || (!d_indices && capacity))
+    return fail(SIGMO_ERR_INVALID, "sigmo_gmcr_generate_noalloc: null argument");
+  if (c->rows != query->total_nodes || c->targets != data->total_nodes)
+    return fail(SIGMO_ERR_INVALID, "candidate bitset does not match the graphs");
+  SIGMO_CUDA_TRY(cudaSetDevice(q->device));
+  const uint32_t G = data->num_graphs, QG = query->num_graphs, GW = (G + 31u) / 32u;
+  const uint64_t Qn = query->total_nodes;
+  size_t cub_bytes = 0;
+  if (G)
+    SIGMO_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, cub_bytes, static_cast<uint32_t*>(nullptr),
+                                                 static_cast<uint32_t*>(nullptr), static_cast<int>(G), q->stream));
+  auto al = [](size_t x) { return (x + 255) & ~static_cast<size_t>(255); };
+  const size_t need = al(4ull * Qn * GW) + al(4ull * QG * GW) + al(4ull * G) + al(cub_bytes);
+  if (need > kNoAllocScratchBytes)
+    return fail(SIGMO_ERR_DOMAIN,
+                "sigmo_gmcr_generate_noalloc: %zu bytes of scratch needed (%llu query vertices x %u data graphs), the "
+                "static scratch holds %zu; use sigmo_gmcr_generate",
+                need, static_cast<unsigned long long>(Qn), G, kNoAllocScratchBytes);
+  void* scratch = nullptr;
+  SIGMO_TRY(noalloc_scratch(q->device, &scratch));
+  char* p = static_cast<char*>(scratch);
+  uint32_t* NE = reinterpret_cast<uint32_t*>(p);
+  p += al(4ull * Qn * GW);
+  uint32_t* admit = reinterpret_cast<uint32_t*>(p);
+  p += al(4ull * QG * GW);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(p);
+  p += al(4ull * G);
+  void* cub_tmp = p;
+  // d_offsets[0] must start at zero; NE, admit and counts are fully written below.
+  SIGMO_CUDA_TRY(cudaMemsetAsync(d_offsets, 0, sizeof(uint32_t) * (G + 1ull), q->stream));
+  if (G && QG && Qn) {
+    dim3 grid_ne((GW + 7u) / 8u, static_cast<unsigned>((Qn + kNeRowsPerBlock - 1) / kNeRowsPerBlock));
+    if (grid_ne.y > 65535u) return fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", static_cast<unsigned long long>(Qn));
+    k_gmcr_ne<<<grid_ne, 256, 0, q->stream>>>(c->bits, c->Wp, Qn, data->graph_offsets, G, GW, q->opts.profile, NE);
+    SIGMO_TRY(check_launch(q, "k_gmcr_ne"));
+    k_gmcr_admit<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(NE, GW, query->graph_offsets, QG, G, nullptr,
+                                                                                admit, counts);
+    SIGMO_TRY(check_launch(q, "k_gmcr_admit"));
+    SIGMO_CUDA_TRY(cub::DeviceScan::InclusiveSum(cub_tmp, cub_bytes, counts, d_offsets + 1, static_cast<int>(G), q->stream));
+    q->launches += 2;
+  }
+  uint32_t* pinned = static_cast<uint32_t*>(q->pinned);
+  SIGMO_CUDA_TRY(cudaMemcpyAsync(pinned, d_offsets + G, sizeof(uint32_t), cudaMemcpyDeviceToHost, q->stream));
+  SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));
+  *total = *pinned;
+  if (*total > capacity)
+    return fail(SIGMO_ERR_INVALID, "sigmo_gmcr_generate_noalloc: %llu admitted pairs exceed the index buffer of %llu entries",
+                static_cast<unsigned long long>(*total), static_cast<unsigned long long>(capacity));
+  if (G && QG && Qn) {
+    k_gmcr_fill<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(admit, GW, QG, G, d_offsets, d_indices, nullptr,
+                                                                                capacity);
+    SIGMO_TRY(check_launch(q, "k_gmcr_fill"));
+  }
+  return SIGMO_OK;
+}
