@@ -219,10 +219,9 @@ def join_bytes(q, d, offsets, indices):
 def refine_bytes(Qn, N):
     """Algorithmic bytes of one plain refinement pass: the bitset read and
     written once (4 B per 32 (query vertex, data vertex) pairs each way), the
-    thermometer planes of the data signatures (16 labels x 15 counts x 4 B
-    per 32 data vertices) and the query signatures read once."""
+    data and query signatures read once (8 B per vertex)."""
     W = (N + 31) // 32
-    return 8 * Qn * W + 16 * 15 * 4 * W + 8 * Qn
+    return 8 * Qn * W + 8 * N + 8 * Qn
 
 
 def fused_filter_bytes(Qn, N, R):
@@ -353,7 +352,7 @@ def run_sigmo(args, rank, world, local):
         plain = {"value": pairs / (p_ms / 1e3), "unit": "pairs/s", "ms_per_step": round(p_ms, 3),
                  "batched_over_plain": round((pairs / (ms_per_step / 1e3)) / (pairs / (p_ms / 1e3)), 3),
                  "identical_results": bool(p_total == total_matches and p_adm == admitted),
-                 "roofline_refine": {"kernel": "k_sig_thermo + k_refine (one refinement pass)", "bound": "hbm",
+                 "roofline_refine": {"kernel": "k_sig_planes + k_refine (one refinement pass)", "bound": "hbm",
                                      "achieved": round(r_ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(r_ach / hbm, 4),
                                      "traffic": traffic_for("k_refine", args.workload),
                                      "algorithmic_bytes_per_launch": rb, "ms_per_launch": round(r_ms, 4)}}

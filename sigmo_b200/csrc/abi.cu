@@ -530,15 +530,15 @@ int sigmo_refine_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t 
   if (!s->data_planes || s->planes_Wp != c->Wp) {
     dev_free(q, s->data_planes);
     s->data_planes = nullptr;
-    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&s->data_planes), 4ull * 16 * 15 * c->Wp));
+    SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&s->data_planes), 16ull * 16 * c->Wp));
     s->planes_Wp = c->Wp;
     s->planes_valid = false;
   }
   if (!s->planes_valid) {
-    SIGMO_TRY(launch_sig_thermo(q, s->data_sig, s->data_nodes, c->Wp, s->data_planes));
+    SIGMO_TRY(launch_sig_planes(q, s->data_sig, s->data_nodes, c->Wp, s->data_planes));
     s->planes_valid = true;
   }
-  SIGMO_TRY(launch_refine(q, query, data, s->query_sig, s->data_planes, c));
+  SIGMO_TRY(launch_refine(q, s->query_sig, s->data_planes, c));
   return stage_end(q);
 }
 

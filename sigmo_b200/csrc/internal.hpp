@@ -100,7 +100,7 @@ struct Signature {
   uint64_t* data_reach = nullptr;
   uint64_t* query_reach = nullptr;
   uint32_t reach_words = 1;  // 1 (REF_PTX) or 4 (EXACT)
-  uint32_t* data_planes = nullptr;  // thermometer planes of the data signatures [16*15][Wp]
+  uint32_t* data_planes = nullptr;  // bit-sliced data signatures [16][Wp] x uint4 (k_sig_planes)
   uint64_t planes_Wp = 0;
   bool planes_valid = false;
 };
@@ -142,10 +142,8 @@ int launch_sig_generate(Queue* q, const Graph* g, uint64_t* sig);
 int launch_sig_refine(Queue* q, const Graph* g, uint32_t view, uint64_t* sig, uint64_t* reach, uint32_t reach_words);
 int launch_sig_all(Queue* q, const Graph* g, uint32_t R, uint64_t* sig_all /* [R][N] */);
 int launch_sig_planes(Queue* q, const uint64_t* sig, uint64_t n, uint64_t Wp, uint32_t* planes);
-int launch_sig_thermo(Queue* q, const uint64_t* sig, uint64_t n, uint64_t Wp, uint32_t* therm);
 int launch_filter(Queue* q, const Graph* query, const Graph* data, Candidates* c);
-int launch_refine(Queue* q, const Graph* query, const Graph* data, const uint64_t* qsig, const uint32_t* therm,
-                  Candidates* c);
+int launch_refine(Queue* q, const uint64_t* qsig, const uint32_t* planes, Candidates* c);
 int launch_fused_filter(Queue* q, const Graph* query, const Graph* data, uint32_t R, const uint64_t* qsig_all,
                         const uint32_t* planes_all, Candidates* c);
 int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, bool sync_total,

@@ -21,32 +21,46 @@
 namespace sigmo_b200 {
 namespace {
 
-constexpr unsigned kNeRowsPerBlock = 32;
+constexpr unsigned kNeRowsPerBlock = 64;
+constexpr unsigned kNeBatch = 8;  // rows whose words are loaded together
 
-__device__ __forceinline__ bool range_nonempty(const uint32_t* __restrict__ row, uint32_t s, uint32_t e, int prof) {
-  const uint32_t i0 = s >> 5, i1 = (e + 31u) >> 5;
-  for (uint32_t i = i0; i < i1; ++i)
-    if (row[i] & range_mask(i, s, e, prof)) return true;
-  return false;
-}
-
+// Lane = data graph, warp = 32 consecutive graphs (their words are
+// contiguous, so a warp's loads for one row cover ~35 consecutive words).
+// kNeBatch rows are read per pass over the graph's words so that many loads
+// are in flight per lane.
 __global__ void k_gmcr_ne(const uint32_t* __restrict__ bits, uint64_t Wp, uint64_t Qn, const uint32_t* __restrict__ dgoff,
                           uint32_t G, uint32_t GW, int prof, uint32_t* __restrict__ NE) {
   const unsigned lane = threadIdx.x & 31u;
   const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (gw >= GW) return;
   const uint32_t g = gw * 32u + lane;
-  uint32_t s = 0, e = 0;
+  uint32_t s = 0, e = 0, i0 = 0, i1 = 0;
   if (g < G) {
     s = dgoff[g];
     e = dgoff[g + 1];
+    if (e > s) {
+      i0 = s >> 5;
+      i1 = (e + 31u) >> 5;
+    }
   }
   const uint64_t j0 = static_cast<uint64_t>(blockIdx.y) * kNeRowsPerBlock;
   const uint64_t j1 = j0 + kNeRowsPerBlock < Qn ? j0 + kNeRowsPerBlock : Qn;
-  for (uint64_t j = j0; j < j1; ++j) {
-    const bool ne = g < G && range_nonempty(bits + j * Wp, s, e, prof);
-    const uint32_t word = __ballot_sync(0xFFFFFFFFu, ne);
-    if (lane == 0) NE[j * GW + gw] = word;
+  for (uint64_t j = j0; j < j1; j += kNeBatch) {
+    uint32_t acc[kNeBatch];
+#pragma unroll
+    for (uint32_t k = 0; k < kNeBatch; ++k) acc[k] = 0;
+    for (uint32_t i = i0; i < i1; ++i) {
+      const uint32_t m = range_mask(i, s, e, prof);
+      const uint32_t* col = bits + j * Wp + i;
+#pragma unroll
+      for (uint32_t k = 0; k < kNeBatch; ++k)
+        if (j + k < j1) acc[k] |= col[k * Wp] & m;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < kNeBatch; ++k) {
+      const uint32_t word = __ballot_sync(0xFFFFFFFFu, acc[k] != 0);
+      if (lane == 0 && j + k < j1) NE[(j + k) * GW + gw] = word;
+    }
   }
 }
 
