@@ -20,7 +20,9 @@ void free_program(Queue* q, PlaneProgram* pp) {
   dev_free(q, pp->prog_off);
   dev_free(q, pp->prog);
   dev_free(q, pp->cls);
-  dev_free(q, pp->cp);
+  dev_free(q, pp->r_begin);
+  dev_free(q, pp->trie);
+  dev_free(q, pp->segs);
   dev_free(q, pp->qsig_all);
   *pp = PlaneProgram{};
 }
@@ -78,8 +80,7 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
 
   // classes: distinct (label, sig_1..sig_R); program = label plane, then the
   // thresholds in (r, l) order.  Classes are numbered in lexicographic order
-  // of their programs so consecutive classes share prefixes; cp[c] = length
-  // of the prefix class c shares with class c-1.
+  // of their programs, which is also the preorder of the programs' trie.
   std::map<std::vector<uint16_t>, uint32_t> programs;  // program -> class
   std::vector<uint16_t> cur;
   std::vector<std::vector<uint16_t>> prog_of_vertex(Qn);
@@ -96,29 +97,115 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   }
   std::vector<uint32_t> cls(Qn), prog_off{0};
   std::vector<uint16_t> prog;
-  std::vector<uint8_t> cp;
-  const std::vector<uint16_t>* prev = nullptr;
   uint32_t max_len = 0;
+  // trie nodes in preorder
+  struct TNode {
+    uint32_t plane, depth, parent, cls, nchild;
+  };
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  std::vector<TNode> nodes;
+  std::vector<uint32_t> path;  // node index per depth along the current program
+  const std::vector<uint16_t>* prev = nullptr;
   for (auto& kv : programs) {
-    kv.second = static_cast<uint32_t>(cp.size());
+    const uint32_t c = static_cast<uint32_t>(prog_off.size() - 1);
+    kv.second = c;
+    const std::vector<uint16_t>& pr = kv.first;
     uint32_t common = 0;
     if (prev)
-      while (common < prev->size() && common < kv.first.size() && (*prev)[common] == kv.first[common]) ++common;
-    cp.push_back(static_cast<uint8_t>(common < 255 ? common : 255));
-    prog.insert(prog.end(), kv.first.begin(), kv.first.end());
+      while (common < prev->size() && common < pr.size() && (*prev)[common] == pr[common]) ++common;
+    path.resize(common);
+    for (uint32_t d = common; d < pr.size(); ++d) {
+      const uint32_t parent = d ? path[d - 1] : kNone;
+      if (parent != kNone) ++nodes[parent].nchild;
+      path.push_back(static_cast<uint32_t>(nodes.size()));
+      nodes.push_back(TNode{pr[d], d, parent, kNone, 0});
+    }
+    nodes[path[pr.size() - 1]].cls = c;
+    prog.insert(prog.end(), pr.begin(), pr.end());
     prog_off.push_back(static_cast<uint32_t>(prog.size()));
-    max_len = std::max<uint32_t>(max_len, static_cast<uint32_t>(kv.first.size()));
-    prev = &kv.first;
+    max_len = std::max<uint32_t>(max_len, static_cast<uint32_t>(pr.size()));
+    prev = &pr;
   }
   for (uint64_t v = 0; v < Qn; ++v) cls[v] = programs[prog_of_vertex[v]];
-  std::map<std::vector<uint16_t>, uint32_t>& classes = programs;
+  const uint32_t C = static_cast<uint32_t>(prog_off.size() - 1);
+  // node codes (layout documented at k_planes_ne), skip pointers, segments
+  const uint32_t n = static_cast<uint32_t>(nodes.size());
+  std::vector<uint32_t> branch_above(n, 0), skip(n, n);
+  uint32_t max_slot = 0;
+  std::vector<uint4> trie(n);
+  {
+    std::vector<uint32_t> open;
+    for (uint32_t i = 0; i < n; ++i) {
+      while (!open.empty() && nodes[open.back()].depth >= nodes[i].depth) {
+        skip[open.back()] = i;
+        open.pop_back();
+      }
+      open.push_back(i);
+    }
+  }
+  // Plane and stack offsets are stored as row indices (a row is AW words of
+  // 32 graphs); the kernel scales them by its AW.
+  for (uint32_t i = 0; i < n; ++i) {
+    const TNode& t = nodes[i];
+    if (t.parent != kNone) branch_above[i] = branch_above[t.parent] + (nodes[t.parent].nchild >= 2 ? 1u : 0u);
+    if (t.nchild >= 2) max_slot = std::max(max_slot, branch_above[i]);
+  }
+  const uint32_t root_slot = max_slot + 1;
+  for (uint32_t i = 0; i < n; ++i) {
+    const TNode& t = nodes[i];
+    uint32_t x = t.plane, rd = 0, wr = 0;
+    if (t.nchild >= 2) {
+      x |= 1u << 21;
+      wr = branch_above[i];
+    }
+    if (t.parent == kNone) {
+      x |= 1u << 20;
+      rd = root_slot;
+    } else if (t.parent != i - 1) {
+      x |= 1u << 20;  // the parent is a branch node, its mask is on the stack
+      rd = branch_above[t.parent];
+    }
+    if (t.cls != kNone) x |= 1u << 22;
+    trie[i] = make_uint4(x, skip[i], t.cls == kNone ? 0u : t.cls, rd | (wr << 16));
+  }
+  const bool trie_ok = root_slot < 32;
+  std::vector<uint4> segs;
+  {
+    const uint32_t target = std::max<uint32_t>(32u, n / 96u);
+    uint32_t begin = 0;
+    auto close = [&](uint32_t end) {
+      if (end <= begin) return;
+      uint32_t z = 0;
+      if (nodes[begin].depth == 1) {
+        const uint32_t p = nodes[begin].parent;
+        z = 0x80000000u | nodes[p].plane | (nodes[p].nchild >= 2 ? (1u << 21) : 0u);
+      }
+      segs.push_back(make_uint4(begin, end, z, 0u));
+      begin = end;
+    };
+    for (uint32_t i = 1; i < n; ++i)
+      if (nodes[i].depth <= 1 && i - begin >= target) close(i);
+    close(n);
+  }
+  std::vector<uint32_t> r_begin(R + 1, static_cast<uint32_t>(spec.size()));
+  for (uint32_t k = static_cast<uint32_t>(label_plane.size()); k < spec.size(); ++k) {
+    const uint32_t r = (spec[k] >> 16) & 0xFFu;
+    r_begin[r] = std::min(r_begin[r], k);
+  }
+  for (int r = static_cast<int>(R) - 1; r >= 0; --r) r_begin[r] = std::min(r_begin[r], r_begin[r + 1]);
   pp.K = static_cast<uint32_t>(spec.size());
-  pp.C = static_cast<uint32_t>(classes.size());
+  pp.C = C;
+  pp.nlab = static_cast<uint32_t>(label_plane.size());
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.spec), spec.data(), 4 * spec.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog_off), prog_off.data(), 4 * prog_off.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog), prog.data(), 2 * prog.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.cls), cls.data(), 4 * cls.size()));
-  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.cp), cp.data(), cp.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.r_begin), r_begin.data(), 4 * r_begin.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.trie), trie.data(), 16 * trie.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.segs), segs.data(), 16 * segs.size()));
+  pp.trie_n = n;
+  pp.nsegs = static_cast<uint32_t>(segs.size());
+  pp.nslots = trie_ok ? root_slot + 1 : 0xFFFFFFFFu;
   pp.max_len = max_len;
   SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
   pp.R = R;
@@ -258,7 +345,7 @@ extern "C" int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_g
   uint64_t* d_total = nullptr;
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
   int rc = cudaMemsetAsync(d_total, 0, 8, q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "memset failed");
-  const bool planes_fit = ne_planes_smem(query->pp.K, data->adj_words) <= 200u * 1024u;
+  const bool planes_fit = query->pp.nslots <= 32u && ne_planes_smem(query->pp.K, data->adj_words, query->pp.nslots) <= 200u * 1024u;
   if (!rc) {
     if (materialize || !planes_fit) {
       sigmo_candidates_t cc = c;

@@ -52,7 +52,13 @@ struct PlaneProgram {
   uint32_t* prog_off = nullptr;   // [C + 1]
   uint16_t* prog = nullptr;       // plane indices of each class's program
   uint32_t* cls = nullptr;        // [query vertices] class of each vertex
-  uint8_t* cp = nullptr;          // [C] prefix shared with the previous class's program
+  uint32_t nlab = 0;              // label planes (spec[0 .. nlab))
+  uint32_t* r_begin = nullptr;    // [R + 1] first threshold plane of each iteration
+  uint4* trie = nullptr;          // [trie_n] preorder trie of the class programs {code, skip, class, 0}
+  uint32_t trie_n = 0;
+  uint4* segs = nullptr;          // [nsegs] walk segments {begin, end, parent code, 0}
+  uint32_t nsegs = 0;
+  uint32_t nslots = 0;            // mask stack slots per warp (branch nesting depth)
   uint32_t max_len = 0;           // longest program
   uint64_t* qsig_all = nullptr;   // [R][query vertices] signatures, iterations 1..R
 };
@@ -158,7 +164,7 @@ int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const u
                         bool sync_total, uint64_t capacity_hint);
 int launch_planes_ne(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
                      uint64_t* planes, uint32_t* NE);
-size_t ne_planes_smem(uint32_t K, uint32_t AW);
+size_t ne_planes_smem(uint32_t K, uint32_t AW, uint32_t nslots);
 int launch_fused_filter_raw(Queue* q, const uint8_t* qlab, const uint64_t* qsig_all, uint64_t Qn, const uint8_t* dlab,
                             uint64_t N, const uint32_t* planes_all, uint64_t Wstride, uint32_t R, uint32_t* bits);
 int launch_row_counts(Queue* q, const Candidates* c, uint32_t* d_counts);

@@ -26,20 +26,24 @@ namespace {
 
 // spec[k]: bit 31 set = label plane (bits 0..7 = label value, 255 = any);
 // otherwise r = bits 16..23, l = bits 8..15, c = bits 0..7 (count >= c).
+// Label planes come first, then thresholds in (r, l, c) order;
+// r_begin[r] .. r_begin[r + 1] are the thresholds of iteration r.
 
 // One graph's planes into column `gl` of a shared-memory tile [K * AW][32]:
 // the warp's lanes hold vertices lane + 32 p, every plane is a ballot per
-// 32-vertex chunk, and the plane word is stored by a single lane.
+// 32-vertex chunk, and the plane word is stored by a single lane.  Chunks
+// beyond the graph's last vertex are skipped (the warp handles one graph, so
+// that test is uniform).
 template <int AW>
 __device__ __forceinline__ void build_graph_planes(uint64_t* tile, uint32_t gl, uint32_t s, uint32_t e, unsigned lane,
                                                    const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
-                                                   uint64_t N, uint32_t R, uint32_t K, const uint32_t* __restrict__ spec,
-                                                   int prof) {
+                                                   uint64_t N, uint32_t R, uint32_t nlab, const uint32_t* __restrict__ spec,
+                                                   const uint32_t* __restrict__ r_begin, int prof) {
   constexpr int P = 2 * AW;  // 32-vertex chunks per graph
   const uint32_t n = e - s;
+  const uint32_t chunks = (n + 31u) / 32u;
   uint8_t lb[P];
   bool vis[P];
-  uint64_t sg[P][8];  // iterations beyond 8 are re-read from memory
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     const uint32_t t = lane + 32u * p;
@@ -47,143 +51,193 @@ __device__ __forceinline__ void build_graph_planes(uint64_t* tile, uint32_t gl, 
     const uint32_t v = s + t;
     lb[p] = in ? lab[v] : 0;
     vis[p] = in && ((range_mask(v >> 5, s, e, prof) >> (v & 31u)) & 1u);
-#pragma unroll
-    for (int r = 0; r < 8; ++r) sg[p][r] = (in && static_cast<uint32_t>(r) < R) ? sig_all[static_cast<uint64_t>(r) * N + v] : 0ull;
   }
-  for (uint32_t k = 0; k < K; ++k) {
-    const uint32_t sp = spec[k];
-    const bool is_label = (sp & 0x80000000u) != 0;
-    const uint32_t r = (sp >> 16) & 0xFFu, l = (sp >> 8) & 0xFFu, c = sp & 0xFFu;
-    uint32_t chunk[P];
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-      bool pred;
-      const uint32_t t = lane + 32u * p;
-      if (is_label) {
-        const uint32_t val = sp & 0xFFu;
-        pred = vis[p] && (val == kWildcard || lb[p] == val);
-      } else {
-        uint64_t sv = 0;
-        if (r < 8) {
-#pragma unroll
-          for (int rr = 0; rr < 8; ++rr)
-            if (static_cast<uint32_t>(rr) == r) sv = sg[p][rr];
-        } else if (t < n && r < R) {
-          sv = sig_all[static_cast<uint64_t>(r) * N + s + t];
-        }
-        pred = t < n && r < R && sig_get(sv, l) >= c;
-      }
-      chunk[p] = __ballot_sync(0xFFFFFFFFu, pred);
-    }
+  auto put = [&](uint32_t k, const uint32_t (&chunk)[P]) {
 #pragma unroll
     for (int w = 0; w < AW; ++w) {
       const uint64_t word = static_cast<uint64_t>(chunk[2 * w]) | (static_cast<uint64_t>(chunk[2 * w + 1]) << 32);
       if (lane == ((k * AW + w) & 31u)) tile[(k * AW + w) * 32 + gl] = word;
+    }
+  };
+  for (uint32_t k = 0; k < nlab; ++k) {
+    const uint32_t val = spec[k] & 0xFFu;
+    uint32_t chunk[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+      chunk[p] = static_cast<uint32_t>(p) < chunks ? __ballot_sync(0xFFFFFFFFu, vis[p] && (val == kWildcard || lb[p] == val)) : 0u;
+    put(k, chunk);
+  }
+  for (uint32_t r = 0; r < R; ++r) {
+    const uint32_t k0 = r_begin[r], k1 = r_begin[r + 1];
+    if (k0 == k1) continue;
+    uint64_t sg[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const uint32_t t = lane + 32u * p;
+      sg[p] = (static_cast<uint32_t>(p) < chunks && t < n) ? sig_all[static_cast<uint64_t>(r) * N + s + t] : 0ull;
+    }
+    for (uint32_t k = k0; k < k1; ++k) {
+      const uint32_t sp = spec[k];
+      const uint32_t sh = 4u * ((sp >> 8) & 0xFFu), c = sp & 0xFFu;
+      uint32_t chunk[P];
+#pragma unroll
+      for (int p = 0; p < P; ++p)
+        chunk[p] = static_cast<uint32_t>(p) < chunks
+                       ? __ballot_sync(0xFFFFFFFFu, static_cast<uint32_t>((sg[p] >> sh) & 0xFull) >= c)
+                       : 0u;
+      put(k, chunk);
     }
   }
 }
 
 // Per 32-graph tile (one CTA per tile, grid-stride): build the tile's planes
 // in shared memory from the data signatures, write the tile out (coalesced;
-// the join reads it), then NE[class][tile] = ballot over the tile's graphs of
-// "AND of the class's program planes != 0".  Classes are numbered in
-// lexicographic program order and each warp walks a contiguous class range
-// keeping the running prefix ANDs (depth < kPrefix) in shared memory, so a
-// class only ANDs the part of its program it does not share with its
-// predecessor, and a prefix that is empty for all 32 graphs ends every class
-// below it at once.
-constexpr uint32_t kPrefix = 16;
+// the join reads it), then walk the trie of the class programs:
+// NE[class][tile] = ballot over the tile's graphs of "AND of the class's
+// program planes != 0".
+//
+// The trie (host-built, preorder) stores per node a uint4 {x, skip, class, y}:
+//   x bits 0..19  the node's plane (row index in the tile)
+//     bit  20     the parent mask is read from the stack (else it is the
+//                 previous node's mask, kept in registers)
+//     bit  21     branch node (two or more children): save the mask
+//     bit  22     terminal: `class` is the class whose program ends here
+//   y bits 0..15  stack slot to read the parent mask from
+//     bits 16..31 stack slot to save this node's mask to
+//   skip          the preorder index after this node's subtree
+// A node whose mask is zero in all 32 graphs jumps to `skip`, so every class
+// below a dead prefix is skipped (NE is zeroed beforehand).  A branch node's
+// slot is its number of branch ancestors, so a saved mask is never
+// overwritten while its later children can still read it; the last slot
+// holds all ones and is the parent of the top-level nodes.
+//
+// The walk is split into segments starting at nodes of depth <= 1 (seg =
+// {begin, end, z}); warps take segments of the tile from a shared counter.
+// A segment starting at depth 1 first evaluates its parent, a top-level
+// plane (z bit 31; z bits 0..19 its row, z bit 21 save it to slot 0).
+// Each warp keeps a 32-node window of the trie in registers (one coalesced
+// 16-byte load per lane) and reads it by shuffle.
+constexpr uint32_t kWalkWarps = 16;
+constexpr uint32_t kNodeStackRead = 1u << 20, kNodeBranch = 1u << 21, kNodeTerminal = 1u << 22;
+constexpr uint32_t kNodeOffset = (1u << 20) - 1u;
 
 template <int AW>
-__global__ void __launch_bounds__(256) k_planes_ne(uint32_t G, const uint32_t* __restrict__ goff, const uint8_t* __restrict__ lab,
-                                                  const uint64_t* __restrict__ sig_all, uint64_t N, uint32_t R, uint32_t K,
-                                                  const uint32_t* __restrict__ spec, int prof, uint32_t C,
-                                                  const uint32_t* __restrict__ prog_off, const uint16_t* __restrict__ prog,
-                                                  const uint8_t* __restrict__ cp, uint64_t* __restrict__ planes,
-                                                  uint32_t* __restrict__ NE) {
-  extern __shared__ uint64_t tile[];  // [K * AW][32], then prefix stacks [8 warps][kPrefix][AW][32]
+__global__ void __launch_bounds__(kWalkWarps * 32) k_planes_ne(
+    uint32_t G, const uint32_t* __restrict__ goff, const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
+    uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
+    int prof, const uint4* __restrict__ trie, uint32_t trie_n, const uint4* __restrict__ segs, uint32_t nsegs,
+    uint32_t nslots, uint64_t* __restrict__ planes, uint32_t* __restrict__ NE) {
+  extern __shared__ uint64_t tile[];  // [K * AW][32], then stacks [kWalkWarps][nslots][AW][32]
+  __shared__ uint32_t seg_next;
+  constexpr uint32_t kRow = AW * 32u;  // u64 words per plane row or stack slot
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t GW = (G + 31u) / 32u;
   const uint32_t words = K * AW;
-  uint64_t* pst = tile + static_cast<size_t>(words) * 32 + static_cast<size_t>(wid) * kPrefix * AW * 32;
-  const uint32_t per_warp = (C + nw - 1) / nw;
-  const uint32_t c_begin = wid * per_warp, c_end = c_begin + per_warp < C ? c_begin + per_warp : C;
+  const uint64_t* tl = tile + lane;  // tl[offset + 32 w]: word w of this lane's graph
+  uint64_t* sl = tile + static_cast<size_t>(words) * 32 + static_cast<size_t>(wid) * nslots * AW * 32 + lane;
+#pragma unroll
+  for (int w = 0; w < AW; ++w) sl[((nslots - 1) * AW + w) * 32] = ~0ull;  // the root slot
   for (uint32_t gw = blockIdx.x; gw < GW; gw += gridDim.x) {
     __syncthreads();  // the previous tile is no longer read
     for (uint32_t gl = wid; gl < 32; gl += nw) {
       const uint32_t g = gw * 32u + gl;
       if (g < G) {
-        build_graph_planes<AW>(tile, gl, goff[g], goff[g + 1], lane, lab, sig_all, N, R, K, spec, prof);
+        build_graph_planes<AW>(tile, gl, goff[g], goff[g + 1], lane, lab, sig_all, N, R, nlab, spec, r_begin, prof);
       } else {
         for (uint32_t i = lane; i < words; i += 32) tile[i * 32 + gl] = 0;
       }
     }
+    if (threadIdx.x == 0) seg_next = 0;
     __syncthreads();
     {
       uint4* dst = reinterpret_cast<uint4*>(planes + static_cast<uint64_t>(gw) * words * 32);
       const uint4* src = reinterpret_cast<const uint4*>(tile);
       for (uint32_t i = threadIdx.x; i < words * 16; i += blockDim.x) dst[i] = src[i];
     }
-    uint32_t valid = 0;  // prefix depths held in pst from the previous class
-    for (uint32_t c = c_begin; c < c_end; ++c) {
-      const uint32_t e0 = prog_off[c], len = prog_off[c + 1] - e0;
-      uint32_t d = c == c_begin ? 0u : min(static_cast<uint32_t>(cp[c]), valid);
+    for (;;) {
+      uint32_t si = 0;
+      if (lane == 0) si = atomicAdd(&seg_next, 1u);
+      si = __shfl_sync(0xFFFFFFFFu, si, 0);
+      if (si >= nsegs) break;
+      const uint4 sg = segs[si];
       uint64_t m[AW];
 #pragma unroll
-      for (int w = 0; w < AW; ++w) m[w] = d ? pst[((d - 1) * AW + w) * 32 + lane] : ~0ull;
-      bool alive;
-      {
-        bool any = false;
-#pragma unroll
-        for (int w = 0; w < AW; ++w) any |= m[w] != 0;
-        alive = __any_sync(0xFFFFFFFFu, any);
-      }
-      uint32_t reached = d;
-      for (; d < len && alive; ++d) {
-        const uint32_t k = prog[e0 + d];
-        bool any = false;
+      for (int w = 0; w < AW; ++w) m[w] = ~0ull;
+      if (sg.z & 0x80000000u) {  // the segment starts below a top-level node: evaluate it
 #pragma unroll
         for (int w = 0; w < AW; ++w) {
-          m[w] &= tile[(k * AW + w) * 32 + lane];
-          any |= m[w] != 0;
+          m[w] = tl[(sg.z & kNodeOffset) * kRow + 32 * w];
+          if (sg.z & kNodeBranch) sl[32 * w] = m[w];  // slot 0
         }
-        if (d < kPrefix) {
-#pragma unroll
-          for (int w = 0; w < AW; ++w) pst[(d * AW + w) * 32 + lane] = m[w];
-        }
-        reached = d + 1;
-        alive = __any_sync(0xFFFFFFFFu, any);
       }
-      valid = reached < kPrefix ? reached : kPrefix;
-      bool any = false;
+      uint32_t i = sg.x, wbase = 0xFFFFFFFFu;
+      uint4 win = make_uint4(0, 0, 0, 0);
+      while (i < sg.y) {
+        if (i < wbase || i - wbase >= 32u) {
+          wbase = i;
+          win = i + lane < trie_n ? trie[i + lane] : make_uint4(0, 0, 0, 0);
+        }
+        const uint32_t at = i - wbase;
+        const uint32_t x = __shfl_sync(0xFFFFFFFFu, win.x, at);
+        const uint32_t y = __shfl_sync(0xFFFFFFFFu, win.w, at);
+        const uint32_t off = (x & kNodeOffset) * kRow;
+        bool any = false;
+        if (x & kNodeStackRead) {
 #pragma unroll
-      for (int w = 0; w < AW; ++w) any |= m[w] != 0;
-      const uint32_t word = __ballot_sync(0xFFFFFFFFu, alive && any);
-      if (lane == 0) NE[static_cast<uint64_t>(c) * GW + gw] = word;
+          for (int w = 0; w < AW; ++w) {
+            m[w] = sl[(y & 0xFFFFu) * kRow + 32 * w] & tl[off + 32 * w];
+            any |= m[w] != 0;
+          }
+        } else {
+#pragma unroll
+          for (int w = 0; w < AW; ++w) {
+            m[w] &= tl[off + 32 * w];
+            any |= m[w] != 0;
+          }
+        }
+        if (!__any_sync(0xFFFFFFFFu, any)) {
+          i = __shfl_sync(0xFFFFFFFFu, win.y, at);  // past this node's subtree
+          continue;
+        }
+        if (x & kNodeBranch) {
+#pragma unroll
+          for (int w = 0; w < AW; ++w) sl[(y >> 16) * kRow + 32 * w] = m[w];
+        }
+        if (x & kNodeTerminal) {
+          const uint32_t cls = __shfl_sync(0xFFFFFFFFu, win.z, at);
+          const uint32_t word = __ballot_sync(0xFFFFFFFFu, any);
+          if (lane == 0) NE[static_cast<uint64_t>(cls) * GW + gw] = word;
+        }
+        ++i;
+      }
     }
   }
 }
 
 }  // namespace
 
-size_t ne_planes_smem(uint32_t K, uint32_t AW) {
-  return static_cast<size_t>(K) * AW * 32 * 8 + static_cast<size_t>(8) * kPrefix * AW * 32 * 8;
+size_t ne_planes_smem(uint32_t K, uint32_t AW, uint32_t nslots) {
+  return static_cast<size_t>(K) * AW * 32 * 8 + static_cast<size_t>(kWalkWarps) * nslots * AW * 32 * 8;
 }
 
 int launch_planes_ne(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
                      uint64_t* planes, uint32_t* NE) {
   const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u;
   if (!GW) return SIGMO_OK;
-  const size_t smem = ne_planes_smem(pp.K, data->adj_words);
-  const unsigned block = 256;
-  const unsigned grid = std::min<uint32_t>(GW, 148u * 8u);
+  SIGMO_CUDA_TRY(cudaMemsetAsync(NE, 0, 4ull * pp.C * GW, q->stream));
+  const size_t smem = ne_planes_smem(pp.K, data->adj_words, pp.nslots);
+  const unsigned block = 32u * kWalkWarps;
   cudaError_t e = cudaSuccess;
-#define SIGMO_PLANES_NE(AWV)                                                                                             \
-  e = cudaFuncSetAttribute(k_planes_ne<AWV>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));      \
-  if (e == cudaSuccess)                                                                                                  \
-    k_planes_ne<AWV><<<grid, block, smem, q->stream>>>(G, data->graph_offsets, data->node_labels, sig_all,              \
-                                                      data->total_nodes, R, pp.K, pp.spec, q->opts.profile, pp.C,      \
-                                                      pp.prog_off, pp.prog, pp.cp, planes, NE)
+  int per_sm = 0, sms = 0;
+  SIGMO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device));
+#define SIGMO_PLANES_NE(AWV)                                                                                          \
+  e = cudaFuncSetAttribute(k_planes_ne<AWV>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));   \
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_planes_ne<AWV>, block, smem);    \
+  if (e == cudaSuccess)                                                                                               \
+    k_planes_ne<AWV><<<std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms), block, smem,          \
+                       q->stream>>>(G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, pp.K,   \
+                                    pp.nlab, pp.spec, pp.r_begin, q->opts.profile, pp.trie, pp.trie_n, pp.segs,       \
+                                    pp.nsegs, pp.nslots, planes, NE)
   switch (data->adj_words) {
     case 1: SIGMO_PLANES_NE(1); break;
     case 2: SIGMO_PLANES_NE(2); break;
