@@ -68,6 +68,10 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=10_000, help="molecules in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mols", type=int, default=0, help="override the workload's molecule count (profiling runs)")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the serving run (0: skip it)")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="mean request arrivals per second (Poisson)")
+    ap.add_argument("--serve-mols", type=int, default=0, help="serving database size (0: the workload's molecules)")
+    ap.add_argument("--serve-inflight", type=int, default=2)
     return ap.parse_args()
 
 
@@ -233,6 +237,76 @@ def fused_filter_bytes(Qn, N, R):
     W = (N + 31) // 32
     Wp = (W + 31) // 32 * 32
     return 4 * Qn * Wp + N + R * 16 * 16 * Wp + 8 * R * Qn + Qn
+
+
+# ---- serving loop ---------------------------------------------------------------------
+def run_serving(args, d, wl, local):
+    """Poisson arrivals (mean `--serve-rate` per second) of requests of 1-64
+    query graphs (3-30 atoms, skewed 6-15) against the resident database,
+    find-first, continuous batching; latency = submit -> per-query results on
+    the host, measured inside the library."""
+    import threading
+
+    import sigmo_b200 as sb
+
+    if args.serve_mols and args.serve_mols != d.num_graphs:
+        d = sb.generate_molecules(args.serve_mols, wl["min_atoms"], wl["max_atoms"], seed=wl["seed_d"] + 17, kind=wl["kind"],
+                                  median=wl["median"])
+    rng = np.random.default_rng(4242)
+    n_req = max(1, int(round(args.serve_rate * args.serve_seconds)))
+    sizes = rng.integers(1, 65, n_req)
+    reqs = [sb.generate_queries(int(k), 3, 30, seed=700_000 + i, skew_lo=6, skew_hi=15) for i, k in enumerate(sizes)]
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
+    t_setup = time.perf_counter()
+    srv = sb.Server(d, device=local, iterations=wl["R"], find_first=True, max_inflight=args.serve_inflight,
+                    max_batch_queries=64)
+    setup_s = time.perf_counter() - t_setup
+    # warm-up: a few requests before the timed arrivals
+    for t in [srv.submit(reqs[i % n_req]) for i in range(4)]:
+        srv.wait(t)
+        srv.release(t)
+    tickets = [None] * n_req
+
+    def submitter():
+        t0 = time.perf_counter()
+        for i in range(n_req):
+            delay = arrivals[i] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets[i] = srv.submit(reqs[i])
+
+    st0 = srv.stats()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        results = [srv.wait(t) for t in tickets]
+        wall = time.perf_counter() - t0
+    st1 = srv.stats()
+    srv.close()
+    lat = np.array([r["ms_latency"] for r in results])
+    qms = np.array([r["ms_queue"] for r in results])
+    pairs = sum(r["pairs"] for r in results)
+    big = [r["ms_latency"] for r, k in zip(results, sizes) if k == 64 or r["batch_queries"] >= 48]
+    return {
+        "database": {"molecules": d.num_graphs, "vertices": d.total_nodes, "directed_edges": d.total_edges,
+                     "resident_bytes": st1["resident_bytes"], "setup_s": round(setup_s, 2)},
+        "requests": n_req, "arrival_rate_per_s": args.serve_rate, "queries_per_request": "uniform 1-64",
+        "mode": "find-first", "max_inflight": args.serve_inflight, "max_batch_queries": 64,
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p95": round(float(np.percentile(lat, 95)), 3),
+                       "p99": round(float(np.percentile(lat, 99)), 3), "max": round(float(lat.max()), 3)},
+        "latency_ms_full_batches_p99": round(float(np.percentile(big, 99)), 3) if big else None,
+        "queue_ms_p50": round(float(np.percentile(qms, 50)), 3),
+        "pairs_per_s": round(pairs / wall, 1),
+        "wall_s": round(wall, 3),
+        "batches": st1["batches"] - st0["batches"],
+        "mean_requests_per_batch": round((st1["requests_completed"] - st0["requests_completed"]) /
+                                         max(1, st1["batches"] - st0["batches"]), 2),
+        "max_batches_in_flight": st1["max_batches_in_flight"],
+        "peak_reserved_bytes": st1["peak_reserved_bytes"],
+        "clocks": clk.summary(),
+    }
 
 
 # ---- the sigmo arm -------------------------------------------------------------------
@@ -410,6 +484,10 @@ def run_sigmo(args, rank, world, local):
                "h2d_bytes_per_step": qbytes + dbytes, "d2h_bytes_per_step": 8 * ea + 8,
                "identical_results": bool(et == total_matches and ea == admitted)}
 
+    serving = None
+    if args.serve_seconds > 0 and world == 1:
+        serving = run_serving(args, d, wl, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(q, d, wl, args.cpu_sample, ff, args.profile)
@@ -449,6 +527,7 @@ def run_sigmo(args, rank, world, local):
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
+        "serving": serving,
     }
     print(json.dumps(out))
 

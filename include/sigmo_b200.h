@@ -262,6 +262,80 @@ SIGMO_API int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_gr
 /* Per-pair counts of the last sigmo_match_batched call on `m` (GMCR slot order). */
 SIGMO_API int sigmo_match_download_counts(sigmo_gmcr_t m, uint64_t* per_pair, uint64_t len);
 
+/* ---- serving loop (no reference counterpart) ----------------------------
+ * The reference answers one query batch per process run (library/src/
+ * sigmo.cpp:98-160).  A server keeps one molecule database resident on the
+ * device (CSR, adjacency rows, signatures of iterations 1..R) and answers
+ * query requests with continuous batching: each of `max_inflight` workers
+ * takes the queued requests in arrival order (up to `max_batch_queries` query
+ * graphs), admits the batch once its projected device footprint fits
+ * `memory_budget` beside the batches already running, and runs the batched
+ * form on its own stream, so batches overlap on the device.  A request's
+ * results are those it gets alone: per (query graph, molecule) pair, the
+ * count of sigmo_match_batched (find-first: 0/1). */
+typedef struct sigmo_server_s* sigmo_server_t;
+
+typedef struct sigmo_server_options {
+  uint32_t iterations;         /* refinement iterations R (default 6)                         */
+  int32_t find_first;          /* 1 (default): per-pair match flags; 0: embedding counts      */
+  uint32_t max_inflight;       /* batches on the device at once, 1..16 (default 2)            */
+  uint32_t max_batch_queries;  /* query graphs per batch (default 64); a larger request runs alone */
+  uint64_t memory_budget;      /* device bytes the running batches may hold (0: half the free memory
+                                  after the database is resident)                              */
+  uint32_t batch_window_us;    /* wait up to this long for a batch to fill (default 0)        */
+} sigmo_server_options;
+
+enum { SIGMO_REQUEST_PAIRS = 1 };  /* keep the matched (query, molecule, count) list */
+
+typedef struct sigmo_request_result {
+  int32_t status;              /* SIGMO_OK or the request's error                              */
+  uint32_t num_queries;
+  uint64_t pairs;              /* num_queries x molecules                                      */
+  uint64_t matched_pairs;      /* pairs with a non-zero count                                  */
+  uint64_t total_matches;      /* sum of the counts (find-first: == matched_pairs)             */
+  uint64_t batch_id;           /* the device batch the request ran in                          */
+  uint32_t batch_queries;      /* query graphs in that batch (all its requests)               */
+  uint32_t batch_requests;
+  uint64_t projected_bytes;    /* the batch's admitted device footprint                        */
+  double ms_queue;             /* submit -> batch start (host clock)                           */
+  double ms_device;            /* the batch's device time (CUDA events)                        */
+  double ms_latency;           /* submit -> results on the host (host clock)                   */
+} sigmo_request_result;
+
+typedef struct sigmo_server_stats {
+  uint64_t requests_submitted, requests_completed, requests_failed, queries_completed;
+  uint64_t batches, pairs, admitted_pairs;
+  double device_ms;                 /* sum over batches                                        */
+  uint64_t peak_reserved_bytes;     /* largest sum of admitted footprints                      */
+  uint32_t max_batches_in_flight;
+  uint32_t pending_requests;
+  uint64_t resident_bytes;          /* database arrays kept on the device                      */
+  uint64_t memory_budget;
+} sigmo_server_stats;
+
+SIGMO_API void sigmo_server_default_options(sigmo_server_options* o);
+/* Uploads the database (copied; the caller keeps `database`) and starts the
+ * workers.  SIGMO_ERR_DOMAIN for molecules of more than 256 atoms. */
+SIGMO_API int sigmo_server_create(int device, const sigmo_host_graphs* database, const sigmo_options* opts,
+                                  const sigmo_server_options* so, sigmo_server_t* out);
+/* Queues a request (the query graphs are copied) and returns at once. */
+SIGMO_API int sigmo_server_submit(sigmo_server_t s, const sigmo_host_graphs* queries, uint32_t flags, uint64_t* ticket);
+/* Waits for a request (timeout_ms < 0: no limit; SIGMO_ERR_TIMEOUT when it
+ * runs out).  Returns the request's own status. */
+SIGMO_API int sigmo_server_wait(sigmo_server_t s, uint64_t ticket, int64_t timeout_ms, sigmo_request_result* out);
+/* Per query graph of a finished request: matched molecules and total count. */
+SIGMO_API int sigmo_server_query_totals(sigmo_server_t s, uint64_t ticket, uint64_t* matched, uint64_t* total, uint32_t n);
+/* Matched pairs of a request submitted with SIGMO_REQUEST_PAIRS, in molecule
+ * then query order (query index within the request); *n receives the count,
+ * min(*n, capacity) entries are copied. */
+SIGMO_API int sigmo_server_pairs(sigmo_server_t s, uint64_t ticket, uint32_t* query, uint32_t* molecule, uint64_t* count,
+                                 uint64_t capacity, uint64_t* n);
+/* Forgets a finished request. */
+SIGMO_API int sigmo_server_release(sigmo_server_t s, uint64_t ticket);
+SIGMO_API int sigmo_server_get_stats(sigmo_server_t s, sigmo_server_stats* out);
+/* Finishes the queued requests, stops the workers, frees the database. */
+SIGMO_API int sigmo_server_destroy(sigmo_server_t s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,7 +34,7 @@ SCOPE_DATA, SCOPE_QUERY = 0, 1
 __all__ = [
     "SigmoError", "HostGraphs", "Queue", "DeviceBatchedCSRGraph", "createDeviceCSRGraph", "destroyDeviceCSRGraph",
     "io", "candidates", "signature", "isomorphism", "generate_molecules", "generate_queries", "match_batched",
-    "REF_PTX", "EXACT",
+    "Server", "REF_PTX", "EXACT",
 ]
 
 
@@ -475,6 +475,84 @@ def match_batched(queue: Queue, query_graphs, data_graphs, iterations: int, find
                                     candidates._h if candidates is not None else None, gmcr._h, ctypes.byref(res)))
     gmcr._num_data_graphs = data_graphs.num_graphs
     return {f: getattr(res, f) for f, _ in _L.MatchResultC._fields_}
+
+
+# ---- serving loop -----------------------------------------------------------------
+REQUEST_PAIRS = 1
+
+
+class Server:
+    """A resident molecule database answering query requests with continuous
+    batching (sigmo_server_*).  `submit` queues a request and returns a ticket
+    at once; `wait` blocks for its result.  Each request's per-pair results
+    are those it gets alone."""
+
+    def __init__(self, database: HostGraphs, device: int = 0, profile="ref-ptx", iterations: int = 6,
+                 find_first: bool = True, max_inflight: int = 2, max_batch_queries: int = 64, memory_budget: int = 0,
+                 batch_window_us: int = 0, join_work_group_size: int = 128):
+        if isinstance(profile, str):
+            profile = PROFILE_NAMES[profile]
+        opts = _L.OptionsC(int(profile), join_work_group_size, 512)
+        so = _L.ServerOptionsC()
+        lib().sigmo_server_default_options(ctypes.byref(so))
+        so.iterations, so.find_first, so.max_inflight = iterations, int(bool(find_first)), max_inflight
+        so.max_batch_queries, so.memory_budget, so.batch_window_us = max_batch_queries, memory_budget, batch_window_us
+        h = ctypes.c_void_p()
+        check(lib().sigmo_server_create(device, ctypes.byref(database._raw), ctypes.byref(opts), ctypes.byref(so),
+                                        ctypes.byref(h)))
+        self._h = h
+        self.num_molecules = database.num_graphs
+
+    def submit(self, queries: HostGraphs, pairs: bool = False) -> int:
+        t = ctypes.c_uint64()
+        check(lib().sigmo_server_submit(self._h, ctypes.byref(queries._raw), REQUEST_PAIRS if pairs else 0, ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> dict:
+        r = _L.RequestResultC()
+        check(lib().sigmo_server_wait(self._h, ticket, timeout_ms, ctypes.byref(r)))
+        return {f: getattr(r, f) for f, _ in _L.RequestResultC._fields_}
+
+    def query_totals(self, ticket: int, num_queries: int):
+        matched = np.zeros(num_queries, np.uint64)
+        total = np.zeros(num_queries, np.uint64)
+        check(lib().sigmo_server_query_totals(self._h, ticket, matched.ctypes.data, total.ctypes.data, num_queries))
+        return matched, total
+
+    def pairs(self, ticket: int):
+        """(query index within the request, molecule, count) of every matched pair."""
+        n = ctypes.c_uint64()
+        check(lib().sigmo_server_pairs(self._h, ticket, None, None, None, 0, ctypes.byref(n)))
+        q = np.zeros(n.value, np.uint32)
+        g = np.zeros(n.value, np.uint32)
+        c = np.zeros(n.value, np.uint64)
+        check(lib().sigmo_server_pairs(self._h, ticket, q.ctypes.data, g.ctypes.data, c.ctypes.data, n.value, ctypes.byref(n)))
+        return q, g, c
+
+    def release(self, ticket: int):
+        check(lib().sigmo_server_release(self._h, ticket))
+
+    def stats(self) -> dict:
+        st = _L.ServerStatsC()
+        check(lib().sigmo_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _L.ServerStatsC._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            check(lib().sigmo_server_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 candidates = SimpleNamespace(Candidates=Candidates)

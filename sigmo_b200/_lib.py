@@ -44,6 +44,52 @@ class MatchResultC(ctypes.Structure):
     ]
 
 
+class ServerOptionsC(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_uint32),
+        ("find_first", ctypes.c_int32),
+        ("max_inflight", ctypes.c_uint32),
+        ("max_batch_queries", ctypes.c_uint32),
+        ("memory_budget", ctypes.c_uint64),
+        ("batch_window_us", ctypes.c_uint32),
+    ]
+
+
+class RequestResultC(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("num_queries", ctypes.c_uint32),
+        ("pairs", ctypes.c_uint64),
+        ("matched_pairs", ctypes.c_uint64),
+        ("total_matches", ctypes.c_uint64),
+        ("batch_id", ctypes.c_uint64),
+        ("batch_queries", ctypes.c_uint32),
+        ("batch_requests", ctypes.c_uint32),
+        ("projected_bytes", ctypes.c_uint64),
+        ("ms_queue", ctypes.c_double),
+        ("ms_device", ctypes.c_double),
+        ("ms_latency", ctypes.c_double),
+    ]
+
+
+class ServerStatsC(ctypes.Structure):
+    _fields_ = [
+        ("requests_submitted", ctypes.c_uint64),
+        ("requests_completed", ctypes.c_uint64),
+        ("requests_failed", ctypes.c_uint64),
+        ("queries_completed", ctypes.c_uint64),
+        ("batches", ctypes.c_uint64),
+        ("pairs", ctypes.c_uint64),
+        ("admitted_pairs", ctypes.c_uint64),
+        ("device_ms", ctypes.c_double),
+        ("peak_reserved_bytes", ctypes.c_uint64),
+        ("max_batches_in_flight", ctypes.c_uint32),
+        ("pending_requests", ctypes.c_uint32),
+        ("resident_bytes", ctypes.c_uint64),
+        ("memory_budget", ctypes.c_uint64),
+    ]
+
+
 _vp, _i, _u32, _u64, _sz, _d = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_double
 _P = ctypes.POINTER
 
@@ -94,6 +140,15 @@ SIGNATURES = {
     "sigmo_gmcr_generate_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _u64, _P(_u64)]),
     "sigmo_join_candidates": (_i, [_vp, _vp, _vp, _vp, _vp, _P(_u64), _i, _vp]),
     "sigmo_match_batched": (_i, [_vp, _vp, _vp, _u32, _i, _u32, _vp, _vp, _P(MatchResultC)]),
+    "sigmo_server_default_options": (None, [_P(ServerOptionsC)]),
+    "sigmo_server_create": (_i, [_i, _P(HostGraphsC), _vp, _P(ServerOptionsC), _P(_vp)]),
+    "sigmo_server_submit": (_i, [_vp, _P(HostGraphsC), _u32, _P(_u64)]),
+    "sigmo_server_wait": (_i, [_vp, _u64, ctypes.c_int64, _P(RequestResultC)]),
+    "sigmo_server_query_totals": (_i, [_vp, _u64, _vp, _vp, _u32]),
+    "sigmo_server_pairs": (_i, [_vp, _u64, _vp, _vp, _vp, _u64, _P(_u64)]),
+    "sigmo_server_release": (_i, [_vp, _u64]),
+    "sigmo_server_get_stats": (_i, [_vp, _P(ServerStatsC)]),
+    "sigmo_server_destroy": (_i, [_vp]),
     "sigmo_match_download_counts": (_i, [_vp, _vp, _u64]),
 }
 

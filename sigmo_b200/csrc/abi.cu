@@ -607,7 +607,7 @@ int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t da
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
   (void)scratch;
   SIGMO_CUDA_TRY(cudaMemsetAsync(d_total, 0, 8, q->stream));
-  int rc = launch_join_literal(q, query, data, c, m, find_first, 0, data->num_graphs, d_total);
+  int rc = launch_join_literal(q, query, data, c, m, find_first, 0, data->num_graphs, d_total, 0, 0xFFFFFFFFu);
   if (!rc) rc = stage_end(q);
   if (!rc) {
     cudaError_t e = cudaMemcpyAsync(q->pinned, d_total, 8, cudaMemcpyDeviceToHost, q->stream);

@@ -232,20 +232,33 @@ struct Events {
   }
 };
 
+// The literal join of graphs [0, L): one launch over every admitted query, or
+// (serving) one per request's query range, so a request's counts do not
+// depend on the other requests of its batch (the reference's work-items
+// carry DFS state from one pair to the next, isomorphism.hpp:309).
+int join_literal_ranges(Queue* q, Graph* query, Graph* data, const Candidates* c, Gmcr* m, int find_first, uint32_t L,
+                        uint64_t* d_total, const BatchedRun& run) {
+  if (!run.query_ranges || run.nranges == 0)
+    return launch_join_literal(q, query, data, c, m, find_first, 0, L, d_total, 0, 0xFFFFFFFFu);
+  for (uint32_t r = 0; r < run.nranges; ++r)
+    SIGMO_TRY(launch_join_literal(q, query, data, c, m, find_first, 0, L, d_total, run.query_ranges[r], run.query_ranges[r + 1]));
+  return SIGMO_OK;
+}
+
 // The bitset route: fused filter writes the final bitset (all words), GMCR
 // and the join read it.  Used when the caller asks for the bitset, or when a
 // batch does not fit the plane route.
 int batched_bitset(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, Candidates* c, Gmcr* m,
-                   uint64_t* d_total, Events& ev) {
+                   uint64_t* d_total, Events& ev, const BatchedRun& run) {
   PlaneProgram& pp = query->pp;
   const uint64_t N = data->total_nodes;
   void* buf = nullptr;
-  const uint64_t b_dsig = 8ull * R * N, b_planes = 16ull * 16 * R * c->Wp;
+  const uint64_t b_dsig = run.dsig ? 0 : 8ull * R * N, b_planes = 16ull * 16 * R * c->Wp;
   auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
   SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + 256));
-  uint64_t* dsig = static_cast<uint64_t*>(buf);
+  uint64_t* dsig = run.dsig ? const_cast<uint64_t*>(run.dsig) : static_cast<uint64_t*>(buf);
   uint32_t* planes = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + al(b_dsig));
-  int rc = launch_sig_all(q, data, R, dsig);
+  int rc = run.dsig ? SIGMO_OK : launch_sig_all(q, data, R, dsig);
   for (uint32_t r = 0; r < R && !rc; ++r)
     rc = launch_sig_planes(q, dsig + static_cast<uint64_t>(r) * N, N, c->Wp, planes + static_cast<uint64_t>(r) * 16 * 4 * c->Wp);
   if (!rc && cudaEventRecord(ev.e[1], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
@@ -254,14 +267,16 @@ int batched_bitset(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   if (!rc) rc = launch_gmcr(q, query, data, c, m, true, 0);
   if (!rc && cudaEventRecord(ev.e[3], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
   const bool exact = q->opts.profile == kProfileExact;
-  if (!rc && !exact) rc = launch_join_literal(q, query, data, c, m, find_first, 0, std::min(data->low_offset_graphs, data->num_graphs), d_total);
+  if (!rc && !exact) rc = join_literal_ranges(q, query, data, c, m, find_first, std::min(data->low_offset_graphs, data->num_graphs),
+                                             d_total, run);
   if (!rc) rc = launch_join_fast(q, query, data, c, m, find_first, d_total);
   dev_free(q, buf);
   return rc;
 }
 
 // The plane route (no full bitset in HBM).
-int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, Gmcr* m, uint64_t* d_total, Events& ev) {
+int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, Gmcr* m, uint64_t* d_total, Events& ev,
+                   const BatchedRun& run) {
   PlaneProgram& pp = query->pp;
   const uint64_t N = data->total_nodes, Qn = query->total_nodes;
   const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, AW = data->adj_words;
@@ -271,12 +286,12 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   const uint64_t Wlow = L ? (static_cast<uint64_t>(data->host_graph_offsets[L]) + 31) / 32 : 0;
   const uint64_t Wlp = (Wlow + 31) / 32 * 32;
   auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-  const uint64_t b_dsig = 8ull * R * N, b_planes = 8ull * GW * pp.K * AW * 32, b_ne = 4ull * pp.C * GW;
+  const uint64_t b_dsig = run.dsig ? 0 : 8ull * R * N, b_planes = 8ull * GW * pp.K * AW * 32, b_ne = 4ull * pp.C * GW;
   const uint64_t b_lplanes = 16ull * 16 * R * Wlp, b_lbits = 4ull * Qn * Wlp;
   void* buf = nullptr;
   SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + al(b_ne) + al(b_lplanes) + al(b_lbits) + 256));
   char* p = static_cast<char*>(buf);
-  uint64_t* dsig = reinterpret_cast<uint64_t*>(p);
+  uint64_t* dsig = run.dsig ? const_cast<uint64_t*>(run.dsig) : reinterpret_cast<uint64_t*>(p);
   p += al(b_dsig);
   uint64_t* planes = reinterpret_cast<uint64_t*>(p);
   p += al(b_planes);
@@ -285,7 +300,7 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   uint32_t* lplanes = reinterpret_cast<uint32_t*>(p);
   p += al(b_lplanes);
   uint32_t* lbits = reinterpret_cast<uint32_t*>(p);
-  int rc = launch_sig_all(q, data, R, dsig);
+  int rc = run.dsig ? SIGMO_OK : launch_sig_all(q, data, R, dsig);
   if (!rc && cudaEventRecord(ev.e[1], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
   if (!rc) rc = launch_planes_ne(q, data, dsig, R, pp, planes, NE);
   if (!rc && cudaEventRecord(ev.e[2], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
@@ -310,7 +325,7 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
     view.W = Wlow;
     view.Wp = Wlp;
     view.bits = lbits;
-    if (!rc) rc = launch_join_literal(q, query, data, &view, m, find_first, 0, L, d_total);
+    if (!rc) rc = join_literal_ranges(q, query, data, &view, m, find_first, L, d_total, run);
     q->stream = main_stream;
   }
   if (!rc) rc = launch_join_fast_planes(q, query, data, pp, planes, m, find_first, d_total);
@@ -323,14 +338,10 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
 
 }  // namespace
 
-extern "C" int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t R, int find_first,
-                                   uint32_t flags, sigmo_candidates_t c, sigmo_gmcr_t m, sigmo_match_result* out) {
-  if (!q || !query || !data || !m || !out) return fail(SIGMO_ERR_INVALID, "null argument");
-  const bool materialize = (flags & SIGMO_MATCH_MATERIALIZE_BITSET) != 0;
-  if (materialize && !c) return fail(SIGMO_ERR_INVALID, "SIGMO_MATCH_MATERIALIZE_BITSET needs a candidates object");
-  if (c && (c->rows != query->total_nodes || c->targets != data->total_nodes))
-    return fail(SIGMO_ERR_INVALID, "candidate bitset does not match the graphs");
-  if (m->q != q || (c && c->q != q) || query->q != q || data->q != q) return fail(SIGMO_ERR_INVALID, "handles belong to another queue");
+namespace sigmo_b200 {
+
+int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, bool materialize, Candidates* c, Gmcr* m,
+                  sigmo_match_result* out, const BatchedRun& run) {
   if (query->max_nodes > kMaxQueryNodes)
     return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
   if (data->max_nodes > 64u * kMaxAdjWords)
@@ -348,12 +359,12 @@ extern "C" int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_g
   const bool planes_fit = query->pp.nslots <= 32u && ne_planes_smem(query->pp.K, data->adj_words, query->pp.nslots) <= 200u * 1024u;
   if (!rc) {
     if (materialize || !planes_fit) {
-      sigmo_candidates_t cc = c;
-      if (!cc) rc = sigmo_candidates_create(q, query->total_nodes, data->total_nodes, &cc);
-      if (!rc) rc = batched_bitset(q, query, data, R, find_first, cc, m, d_total, ev);
+      sigmo_candidates_t cc = static_cast<sigmo_candidates_t>(c);
+      if (!cc) rc = sigmo_candidates_create(static_cast<sigmo_queue_t>(q), query->total_nodes, data->total_nodes, &cc);
+      if (!rc) rc = batched_bitset(q, query, data, R, find_first, cc, m, d_total, ev, run);
       if (cc != c) sigmo_candidates_destroy(cc);
     } else {
-      rc = batched_planes(q, query, data, R, find_first, m, d_total, ev);
+      rc = batched_planes(q, query, data, R, find_first, m, d_total, ev, run);
     }
   }
   if (!rc && cudaEventRecord(ev.e[4], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
@@ -381,4 +392,17 @@ extern "C" int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_g
   }
   dev_free(q, d_total);
   return rc;
+}
+
+}  // namespace sigmo_b200
+
+extern "C" int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t R, int find_first,
+                                   uint32_t flags, sigmo_candidates_t c, sigmo_gmcr_t m, sigmo_match_result* out) {
+  if (!q || !query || !data || !m || !out) return fail(SIGMO_ERR_INVALID, "null argument");
+  const bool materialize = (flags & SIGMO_MATCH_MATERIALIZE_BITSET) != 0;
+  if (materialize && !c) return fail(SIGMO_ERR_INVALID, "SIGMO_MATCH_MATERIALIZE_BITSET needs a candidates object");
+  if (c && (c->rows != query->total_nodes || c->targets != data->total_nodes))
+    return fail(SIGMO_ERR_INVALID, "candidate bitset does not match the graphs");
+  if (m->q != q || (c && c->q != q) || query->q != q || data->q != q) return fail(SIGMO_ERR_INVALID, "handles belong to another queue");
+  return match_batched(q, query, data, R, find_first, materialize, c, m, out, BatchedRun{});
 }

@@ -154,8 +154,9 @@ int launch_fused_filter(Queue* q, const Graph* query, const Graph* data, uint32_
                         const uint32_t* planes_all, Candidates* c);
 int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, bool sync_total,
                 uint64_t capacity_hint);
+// Query graphs [q_begin, q_end) of each segment only (the full range: 0, ~0u).
 int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
-                        uint32_t graph_begin, uint32_t graph_end, uint64_t* d_total);
+                        uint32_t graph_begin, uint32_t graph_end, uint64_t* d_total, uint32_t q_begin, uint32_t q_end);
 int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
                      uint64_t* d_total);
 int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, const PlaneProgram& pp, const uint64_t* planes,
@@ -169,6 +170,18 @@ int launch_fused_filter_raw(Queue* q, const uint8_t* qlab, const uint64_t* qsig_
                             uint64_t N, const uint32_t* planes_all, uint64_t Wstride, uint32_t R, uint32_t* bits);
 int launch_row_counts(Queue* q, const Candidates* c, uint32_t* d_counts);
 int build_plane_program(Queue* q, Graph* query, uint32_t R);
+
+// Options of the batched form beyond the C entry point (the serving loop):
+// data signatures already resident ([R][N], iterations 1..R), and the query
+// graph ranges of the requests batched together (nranges + 1 boundaries) so
+// the literal join of the low-offset graphs runs per request.
+struct BatchedRun {
+  const uint64_t* dsig = nullptr;
+  const uint32_t* query_ranges = nullptr;
+  uint32_t nranges = 0;
+};
+int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, bool materialize, Candidates* c, Gmcr* m,
+                  sigmo_match_result* out, const BatchedRun& run);
 void release_plane_program(Graph* g);
 int launch_digest(Queue* q, const Candidates* c, uint64_t* d_digest);
 

@@ -125,7 +125,7 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
                                const uint32_t* __restrict__ dgoff, const uint64_t* __restrict__ dadj, uint32_t dAW,
                                const uint32_t* __restrict__ droff, const uint32_t* __restrict__ dcol,
                                const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ indices, uint32_t g0,
-                               uint32_t g1, int find_first, uint64_t* __restrict__ counts,
+                               uint32_t g1, uint32_t q_begin, uint32_t q_end, int find_first, uint64_t* __restrict__ counts,
                                unsigned long long* __restrict__ d_total) {
   const uint32_t wg = blockDim.x, lid = threadIdx.x;
   uint64_t my_total = 0;
@@ -135,7 +135,26 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
   for (uint32_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
     const uint32_t s = dgoff[g], e = dgoff[g + 1], ng = e - s;
     const bool small = ng <= 64u;
-    const uint32_t seg0 = offsets[g], seglen = offsets[g + 1] - seg0;
+    // the segment's slots whose query graph is in [q_begin, q_end) (segments
+    // are sorted by query graph, so they are contiguous)
+    uint32_t seg0 = offsets[g], seg1 = offsets[g + 1];
+    if (q_begin != 0 || q_end != 0xFFFFFFFFu) {
+      uint32_t lo = seg0, hi = seg1;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (indices[mid] < q_begin) lo = mid + 1;
+        else hi = mid;
+      }
+      uint32_t lo2 = lo, hi2 = seg1;
+      while (lo2 < hi2) {
+        const uint32_t mid = (lo2 + hi2) >> 1;
+        if (indices[mid] < q_end) lo2 = mid + 1;
+        else hi2 = mid;
+      }
+      seg0 = lo;
+      seg1 = lo2;
+    }
+    const uint32_t seglen = seg1 - seg0;
     uint32_t mapping[kMaxQueryNodes + 1];
 #pragma unroll 1
     for (uint32_t k = 0; k <= kMaxQueryNodes; ++k) mapping[k] = 0;
@@ -566,7 +585,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
 }  // namespace
 
 int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
-                        uint32_t graph_begin, uint32_t graph_end, uint64_t* d_total) {
+                        uint32_t graph_begin, uint32_t graph_end, uint64_t* d_total, uint32_t q_begin, uint32_t q_end) {
   if (graph_end <= graph_begin) return SIGMO_OK;
   if (query->max_nodes > kMaxQueryNodes)
     return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
@@ -581,12 +600,12 @@ int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const C
     k_join_literal<true><<<grid, wg, 0, q->stream>>>(c->bits, c->Wp, q->opts.profile, query->graph_offsets, query->adj,
                                                       data->graph_offsets, data->adj, data->adj_words, data->row_offsets,
                                                       data->column_indices, m->offsets, m->indices, graph_begin, graph_end,
-                                                      find_first, m->counts, tot);
+                                                      q_begin, q_end, find_first, m->counts, tot);
   else
     k_join_literal<false><<<grid, wg, 0, q->stream>>>(c->bits, c->Wp, q->opts.profile, query->graph_offsets, query->adj,
                                                        data->graph_offsets, data->adj, data->adj_words, data->row_offsets,
                                                        data->column_indices, m->offsets, m->indices, graph_begin, graph_end,
-                                                       find_first, m->counts, tot);
+                                                       q_begin, q_end, find_first, m->counts, tot);
   return check_launch(q, "k_join_literal");
 }
 
