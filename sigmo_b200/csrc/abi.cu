@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 
@@ -65,6 +66,8 @@ int set_device(Queue* q) {
 }
 
 int finish_graph(Graph* g) {
+  static std::atomic<uint64_t> next_stamp{1};
+  g->stamp = next_stamp++;
   // max graph size and low-offset count from the host copy of graph_offsets
   uint32_t mx = 0, low = 0;
   for (uint32_t i = 0; i < g->num_graphs; ++i) {

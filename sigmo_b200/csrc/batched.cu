@@ -21,9 +21,10 @@ void free_program(Queue* q, PlaneProgram* pp) {
   dev_free(q, pp->prog);
   dev_free(q, pp->cls);
   dev_free(q, pp->r_begin);
-  dev_free(q, pp->trie);
-  dev_free(q, pp->segs);
+  dev_free(q, pp->qc_off);
+  dev_free(q, pp->qc);
   dev_free(q, pp->qsig_all);
+  pp->qc_off = pp->qc = nullptr;
   *pp = PlaneProgram{};
 }
 
@@ -79,8 +80,7 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   if (spec.size() >= 65535) return fail(SIGMO_ERR_DOMAIN, "query batch needs %zu candidate planes (limit 65535)", spec.size());
 
   // classes: distinct (label, sig_1..sig_R); program = label plane, then the
-  // thresholds in (r, l) order.  Classes are numbered in lexicographic order
-  // of their programs, which is also the preorder of the programs' trie.
+  // thresholds in (r, l) order; classes numbered in lexicographic program order.
   std::map<std::vector<uint16_t>, uint32_t> programs;  // program -> class
   std::vector<uint16_t> cur;
   std::vector<std::vector<uint16_t>> prog_of_vertex(Qn);
@@ -98,95 +98,14 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   std::vector<uint32_t> cls(Qn), prog_off{0};
   std::vector<uint16_t> prog;
   uint32_t max_len = 0;
-  // trie nodes in preorder
-  struct TNode {
-    uint32_t plane, depth, parent, cls, nchild;
-  };
-  constexpr uint32_t kNone = 0xFFFFFFFFu;
-  std::vector<TNode> nodes;
-  std::vector<uint32_t> path;  // node index per depth along the current program
-  const std::vector<uint16_t>* prev = nullptr;
   for (auto& kv : programs) {
-    const uint32_t c = static_cast<uint32_t>(prog_off.size() - 1);
-    kv.second = c;
-    const std::vector<uint16_t>& pr = kv.first;
-    uint32_t common = 0;
-    if (prev)
-      while (common < prev->size() && common < pr.size() && (*prev)[common] == pr[common]) ++common;
-    path.resize(common);
-    for (uint32_t d = common; d < pr.size(); ++d) {
-      const uint32_t parent = d ? path[d - 1] : kNone;
-      if (parent != kNone) ++nodes[parent].nchild;
-      path.push_back(static_cast<uint32_t>(nodes.size()));
-      nodes.push_back(TNode{pr[d], d, parent, kNone, 0});
-    }
-    nodes[path[pr.size() - 1]].cls = c;
-    prog.insert(prog.end(), pr.begin(), pr.end());
+    kv.second = static_cast<uint32_t>(prog_off.size() - 1);
+    prog.insert(prog.end(), kv.first.begin(), kv.first.end());
     prog_off.push_back(static_cast<uint32_t>(prog.size()));
-    max_len = std::max<uint32_t>(max_len, static_cast<uint32_t>(pr.size()));
-    prev = &pr;
+    max_len = std::max<uint32_t>(max_len, static_cast<uint32_t>(kv.first.size()));
   }
   for (uint64_t v = 0; v < Qn; ++v) cls[v] = programs[prog_of_vertex[v]];
   const uint32_t C = static_cast<uint32_t>(prog_off.size() - 1);
-  // node codes (layout documented at k_planes_ne), skip pointers, segments
-  const uint32_t n = static_cast<uint32_t>(nodes.size());
-  std::vector<uint32_t> branch_above(n, 0), skip(n, n);
-  uint32_t max_slot = 0;
-  std::vector<uint4> trie(n);
-  {
-    std::vector<uint32_t> open;
-    for (uint32_t i = 0; i < n; ++i) {
-      while (!open.empty() && nodes[open.back()].depth >= nodes[i].depth) {
-        skip[open.back()] = i;
-        open.pop_back();
-      }
-      open.push_back(i);
-    }
-  }
-  // Plane and stack offsets are stored as row indices (a row is AW words of
-  // 32 graphs); the kernel scales them by its AW.
-  for (uint32_t i = 0; i < n; ++i) {
-    const TNode& t = nodes[i];
-    if (t.parent != kNone) branch_above[i] = branch_above[t.parent] + (nodes[t.parent].nchild >= 2 ? 1u : 0u);
-    if (t.nchild >= 2) max_slot = std::max(max_slot, branch_above[i]);
-  }
-  const uint32_t root_slot = max_slot + 1;
-  for (uint32_t i = 0; i < n; ++i) {
-    const TNode& t = nodes[i];
-    uint32_t x = t.plane, rd = 0, wr = 0;
-    if (t.nchild >= 2) {
-      x |= 1u << 21;
-      wr = branch_above[i];
-    }
-    if (t.parent == kNone) {
-      x |= 1u << 20;
-      rd = root_slot;
-    } else if (t.parent != i - 1) {
-      x |= 1u << 20;  // the parent is a branch node, its mask is on the stack
-      rd = branch_above[t.parent];
-    }
-    if (t.cls != kNone) x |= 1u << 22;
-    trie[i] = make_uint4(x, skip[i], t.cls == kNone ? 0u : t.cls, rd | (wr << 16));
-  }
-  const bool trie_ok = root_slot < 32;
-  std::vector<uint4> segs;
-  {
-    const uint32_t target = std::max<uint32_t>(32u, n / 96u);
-    uint32_t begin = 0;
-    auto close = [&](uint32_t end) {
-      if (end <= begin) return;
-      uint32_t z = 0;
-      if (nodes[begin].depth == 1) {
-        const uint32_t p = nodes[begin].parent;
-        z = 0x80000000u | nodes[p].plane | (nodes[p].nchild >= 2 ? (1u << 21) : 0u);
-      }
-      segs.push_back(make_uint4(begin, end, z, 0u));
-      begin = end;
-    };
-    for (uint32_t i = 1; i < n; ++i)
-      if (nodes[i].depth <= 1 && i - begin >= target) close(i);
-    close(n);
-  }
   std::vector<uint32_t> r_begin(R + 1, static_cast<uint32_t>(spec.size()));
   for (uint32_t k = static_cast<uint32_t>(label_plane.size()); k < spec.size(); ++k) {
     const uint32_t r = (spec[k] >> 16) & 0xFFu;
@@ -201,16 +120,53 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog), prog.data(), 2 * prog.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.cls), cls.data(), 4 * cls.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.r_begin), r_begin.data(), 4 * r_begin.size()));
-  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.trie), trie.data(), 16 * trie.size()));
-  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.segs), segs.data(), 16 * segs.size()));
-  pp.trie_n = n;
-  pp.nsegs = static_cast<uint32_t>(segs.size());
-  pp.nslots = trie_ok ? root_slot + 1 : 0xFFFFFFFFu;
+  pp.h_spec = spec;
+  pp.h_prog = prog;
+  pp.h_prog_off = prog_off;
+  pp.h_cls = cls;
+  pp.h_qgoff = query->host_graph_offsets;
+  pp.qc_for = nullptr;
   pp.max_len = max_len;
   SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
   pp.R = R;
   pp.profile = q->opts.profile;
   pp.valid = true;
+  return SIGMO_OK;
+}
+
+// Per query graph, its distinct classes in the order the admission kernel
+// evaluates them for `data`: rarest label first (the data graphs' vertex
+// counts per label), then longer programs (more thresholds) first, so a
+// query that a graph cannot admit is usually rejected by its first class.
+int order_classes(Queue* q, Graph* query, Graph* data) {
+  PlaneProgram& pp = query->pp;
+  if (pp.qc && pp.qc_for == data && pp.qc_stamp == data->stamp) return SIGMO_OK;
+  SIGMO_TRY(ensure_label_hist(q, data));
+  const uint32_t QG = query->num_graphs;
+  uint64_t all = 0;
+  for (uint64_t x : data->label_hist) all += x;
+  std::vector<uint32_t> off{0}, list, tmp;
+  for (uint32_t qg = 0; qg < QG; ++qg) {
+    tmp.assign(pp.h_cls.begin() + pp.h_qgoff[qg], pp.h_cls.begin() + pp.h_qgoff[qg + 1]);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    auto key = [&](uint32_t c) {
+      const uint32_t lab = pp.h_spec[pp.h_prog[pp.h_prog_off[c]]] & 0xFFu;
+      const uint64_t freq = lab == kWildcard ? all : data->label_hist[lab];
+      return std::make_tuple(freq, 0u - (pp.h_prog_off[c + 1] - pp.h_prog_off[c]), c);
+    };
+    std::sort(tmp.begin(), tmp.end(), [&](uint32_t a, uint32_t b) { return key(a) < key(b); });
+    list.insert(list.end(), tmp.begin(), tmp.end());
+    off.push_back(static_cast<uint32_t>(list.size()));
+  }
+  dev_free(q, pp.qc_off);
+  dev_free(q, pp.qc);
+  pp.qc_off = pp.qc = nullptr;
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.qc_off), off.data(), 4 * off.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.qc), list.data(), 4 * list.size()));
+  SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
+  pp.qc_for = data;
+  pp.qc_stamp = data->stamp;
   return SIGMO_OK;
 }
 
@@ -286,7 +242,8 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   const uint64_t Wlow = L ? (static_cast<uint64_t>(data->host_graph_offsets[L]) + 31) / 32 : 0;
   const uint64_t Wlp = (Wlow + 31) / 32 * 32;
   auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-  const uint64_t b_dsig = run.dsig ? 0 : 8ull * R * N, b_planes = 8ull * GW * pp.K * AW * 32, b_ne = 4ull * pp.C * GW;
+  const uint64_t b_dsig = run.dsig ? 0 : 8ull * R * N, b_planes = 8ull * GW * pp.K * AW * 32,
+                 b_ne = 4ull * query->num_graphs * GW + 4ull * G;
   const uint64_t b_lplanes = 16ull * 16 * R * Wlp, b_lbits = 4ull * Qn * Wlp;
   void* buf = nullptr;
   SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + al(b_ne) + al(b_lplanes) + al(b_lbits) + 256));
@@ -295,16 +252,18 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   p += al(b_dsig);
   uint64_t* planes = reinterpret_cast<uint64_t*>(p);
   p += al(b_planes);
-  uint32_t* NE = reinterpret_cast<uint32_t*>(p);
+  uint32_t* admit = reinterpret_cast<uint32_t*>(p);  // [query graphs][GW], then per-graph counts [G]
+  uint32_t* adm_counts = admit + static_cast<uint64_t>(query->num_graphs) * GW;
   p += al(b_ne);
   uint32_t* lplanes = reinterpret_cast<uint32_t*>(p);
   p += al(b_lplanes);
   uint32_t* lbits = reinterpret_cast<uint32_t*>(p);
   int rc = run.dsig ? SIGMO_OK : launch_sig_all(q, data, R, dsig);
   if (!rc && cudaEventRecord(ev.e[1], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
-  if (!rc) rc = launch_planes_ne(q, data, dsig, R, pp, planes, NE);
+  if (!rc) rc = order_classes(q, query, data);
+  if (!rc) rc = launch_planes_admit(q, query, data, dsig, R, pp, planes, admit, adm_counts);
   if (!rc && cudaEventRecord(ev.e[2], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
-  if (!rc) rc = launch_gmcr_from_ne(q, query, data, NE, pp.cls, m, true, 0);
+  if (!rc) rc = launch_gmcr_from_admit(q, query, data, admit, adm_counts, m, true, 0);
   if (!rc && cudaEventRecord(ev.e[3], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
   const bool literal = !rc && L && m->total;
   if (literal) {
@@ -356,7 +315,7 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   uint64_t* d_total = nullptr;
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
   int rc = cudaMemsetAsync(d_total, 0, 8, q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "memset failed");
-  const bool planes_fit = query->pp.nslots <= 32u && ne_planes_smem(query->pp.K, data->adj_words, query->pp.nslots) <= 200u * 1024u;
+  const bool planes_fit = planes_admit_smem(query->pp.K, data->adj_words, query->pp.C) <= 200u * 1024u;
   if (!rc) {
     if (materialize || !planes_fit) {
       sigmo_candidates_t cc = static_cast<sigmo_candidates_t>(c);

@@ -54,12 +54,16 @@ struct PlaneProgram {
   uint32_t* cls = nullptr;        // [query vertices] class of each vertex
   uint32_t nlab = 0;              // label planes (spec[0 .. nlab))
   uint32_t* r_begin = nullptr;    // [R + 1] first threshold plane of each iteration
-  uint4* trie = nullptr;          // [trie_n] preorder trie of the class programs {code, skip, class, 0}
-  uint32_t trie_n = 0;
-  uint4* segs = nullptr;          // [nsegs] walk segments {begin, end, parent code, 0}
-  uint32_t nsegs = 0;
-  uint32_t nslots = 0;            // mask stack slots per warp (branch nesting depth)
   uint32_t max_len = 0;           // longest program
+  // host copies (class evaluation order)
+  std::vector<uint32_t> h_spec, h_prog_off, h_cls, h_qgoff;
+  std::vector<uint16_t> h_prog;
+  // per query graph, its distinct classes in evaluation order for one data
+  // graph's label frequencies (rebuilt when the data graph changes)
+  uint32_t* qc_off = nullptr;     // [query graphs + 1]
+  uint32_t* qc = nullptr;
+  const void* qc_for = nullptr;   // the data graph the order was built for
+  uint64_t qc_stamp = 0;
   uint64_t* qsig_all = nullptr;   // [R][query vertices] signatures, iterations 1..R
 };
 
@@ -85,6 +89,8 @@ struct Graph {
   uint64_t* qsel = nullptr;        // [total_nodes] adjacency to earlier levels
   uint64_t* qsel_id = nullptr;     // [total_nodes] same, identity order
   std::vector<uint32_t> host_graph_offsets;  // host copy (sizes, dispatch)
+  std::vector<uint64_t> label_hist;          // vertices per label (filled on first use, 256 entries)
+  uint64_t stamp = 0;                        // unique per graph object (cache keys)
   PlaneProgram pp;                 // when this graph is the query side of a batched match
 };
 
@@ -163,9 +169,15 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
                             Gmcr* m, int find_first, uint64_t* d_total);
 int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const uint32_t* NE, const uint32_t* cls, Gmcr* m,
                         bool sync_total, uint64_t capacity_hint);
-int launch_planes_ne(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
-                     uint64_t* planes, uint32_t* NE);
-size_t ne_planes_smem(uint32_t K, uint32_t AW, uint32_t nslots);
+int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
+                        const PlaneProgram& pp, uint64_t* planes, uint32_t* admit, uint32_t* counts);
+size_t planes_admit_smem(uint32_t K, uint32_t AW, uint32_t C);
+// GMCR from admission words admit[query graph][data graph / 32] and the
+// admitted count of every data graph (scan, total, sorted fill).
+int launch_gmcr_from_admit(Queue* q, const Graph* query, const Graph* data, const uint32_t* admit, const uint32_t* counts,
+                           Gmcr* m, bool sync_total, uint64_t capacity_hint);
+// Vertices per label of a graph batch (host copy, computed once).
+int ensure_label_hist(Queue* q, Graph* g);
 int launch_fused_filter_raw(Queue* q, const uint8_t* qlab, const uint64_t* qsig_all, uint64_t Qn, const uint8_t* dlab,
                             uint64_t N, const uint32_t* planes_all, uint64_t Wstride, uint32_t R, uint32_t* bits);
 int launch_row_counts(Queue* q, const Candidates* c, uint32_t* d_counts);

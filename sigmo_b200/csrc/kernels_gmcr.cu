@@ -132,8 +132,8 @@ __global__ void k_gmcr_fill(const uint32_t* __restrict__ admit, uint32_t GW, uin
 // or per class when cls != nullptr).  With sync_total the total is read back
 // and the index arrays sized exactly (the reference reads it back too,
 // gmcr.hpp:80); otherwise capacity_hint bounds them.
-int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const uint32_t* NE, const uint32_t* cls, Gmcr* m,
-                        bool sync_total, uint64_t capacity_hint) {
+int launch_gmcr_from_admit(Queue* q, const Graph* query, const Graph* data, const uint32_t* admit, const uint32_t* counts,
+                           Gmcr* m, bool sync_total, uint64_t capacity_hint) {
   const uint32_t G = data->num_graphs, QG = query->num_graphs;
   const uint32_t GW = (G + 31u) / 32u;
   if (m->offsets && m->num_data_graphs != G) {
@@ -144,28 +144,16 @@ int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const u
   m->num_data_graphs = G;
   m->counts_valid = false;
   SIGMO_CUDA_TRY(cudaMemsetAsync(m->offsets, 0, sizeof(uint32_t) * (G + 1ull), q->stream));
-  const uint64_t admit_words = static_cast<uint64_t>(QG) * GW;
   size_t cub_bytes = 0;
   if (G) cub::DeviceScan::InclusiveSum(nullptr, cub_bytes, static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
                                        static_cast<int>(G), q->stream);
-  auto al = [](size_t x) { return (x + 255) & ~static_cast<size_t>(255); };
-  void* buf = nullptr;
-  SIGMO_TRY(dev_alloc(q, &buf, al(admit_words * 4) + al(G * 4ull) + al(cub_bytes) + 256));
-  char* p = static_cast<char*>(buf);
-  uint32_t* admit = reinterpret_cast<uint32_t*>(p);
-  p += al(admit_words * 4);
-  uint32_t* counts = reinterpret_cast<uint32_t*>(p);
-  p += al(G * 4ull);
-  void* cub_tmp = p;
+  void* cub_tmp = nullptr;
+  SIGMO_TRY(dev_alloc(q, &cub_tmp, cub_bytes + 256));
   int rc = SIGMO_OK;
   if (G && QG) {
-    k_gmcr_admit<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(NE, GW, query->graph_offsets, QG, G, cls, admit, counts);
-    rc = check_launch(q, "k_gmcr_admit");
-    if (!rc) {
-      cudaError_t e = cub::DeviceScan::InclusiveSum(cub_tmp, cub_bytes, counts, m->offsets + 1, static_cast<int>(G), q->stream);
-      if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "device scan failed: %s", cudaGetErrorString(e));
-      q->launches += 2;
-    }
+    cudaError_t e = cub::DeviceScan::InclusiveSum(cub_tmp, cub_bytes, counts, m->offsets + 1, static_cast<int>(G), q->stream);
+    if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "device scan failed: %s", cudaGetErrorString(e));
+    q->launches += 2;
   }
   uint64_t cap = capacity_hint;
   if (!rc && sync_total) {
@@ -194,6 +182,28 @@ int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const u
                                                                                 m->pair_graph, m->capacity);
     rc = check_launch(q, "k_gmcr_fill");
   }
+  dev_free(q, cub_tmp);
+  return rc;
+}
+
+// Admission and counts from an NE matrix (rows per query vertex, or per class
+// when cls != nullptr), then launch_gmcr_from_admit.
+int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const uint32_t* NE, const uint32_t* cls, Gmcr* m,
+                        bool sync_total, uint64_t capacity_hint) {
+  const uint32_t G = data->num_graphs, QG = query->num_graphs;
+  const uint32_t GW = (G + 31u) / 32u;
+  const uint64_t admit_words = static_cast<uint64_t>(QG) * GW;
+  auto al = [](size_t x) { return (x + 255) & ~static_cast<size_t>(255); };
+  void* buf = nullptr;
+  SIGMO_TRY(dev_alloc(q, &buf, al(admit_words * 4) + al(G * 4ull) + 256));
+  uint32_t* admit = static_cast<uint32_t*>(buf);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + al(admit_words * 4));
+  int rc = SIGMO_OK;
+  if (G && QG) {
+    k_gmcr_admit<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(NE, GW, query->graph_offsets, QG, G, cls, admit, counts);
+    rc = check_launch(q, "k_gmcr_admit");
+  }
+  if (!rc) rc = launch_gmcr_from_admit(q, query, data, admit, counts, m, sync_total, capacity_hint);
   dev_free(q, buf);
   return rc;
 }

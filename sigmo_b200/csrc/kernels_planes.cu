@@ -92,51 +92,37 @@ __device__ __forceinline__ void build_graph_planes(uint64_t* tile, uint32_t gl, 
 
 // Per 32-graph tile (one CTA per tile, grid-stride): build the tile's planes
 // in shared memory from the data signatures, write the tile out (coalesced;
-// the join reads it), then walk the trie of the class programs:
-// NE[class][tile] = ballot over the tile's graphs of "AND of the class's
-// program planes != 0".
-//
-// The trie (host-built, preorder) stores per node a uint4 {x, skip, class, y}:
-//   x bits 0..19  the node's plane (row index in the tile)
-//     bit  20     the parent mask is read from the stack (else it is the
-//                 previous node's mask, kept in registers)
-//     bit  21     branch node (two or more children): save the mask
-//     bit  22     terminal: `class` is the class whose program ends here
-//   y bits 0..15  stack slot to read the parent mask from
-//     bits 16..31 stack slot to save this node's mask to
-//   skip          the preorder index after this node's subtree
-// A node whose mask is zero in all 32 graphs jumps to `skip`, so every class
-// below a dead prefix is skipped (NE is zeroed beforehand).  A branch node's
-// slot is its number of branch ancestors, so a saved mask is never
-// overwritten while its later children can still read it; the last slot
-// holds all ones and is the parent of the top-level nodes.
-//
-// The walk is split into segments starting at nodes of depth <= 1 (seg =
-// {begin, end, z}); warps take segments of the tile from a shared counter.
-// A segment starting at depth 1 first evaluates its parent, a top-level
-// plane (z bit 31; z bits 0..19 its row, z bit 21 save it to slot 0).
-// Each warp keeps a 32-node window of the trie in registers (one coalesced
-// 16-byte load per lane) and reads it by shuffle.
-constexpr uint32_t kWalkWarps = 16;
-constexpr uint32_t kNodeStackRead = 1u << 20, kNodeBranch = 1u << 21, kNodeTerminal = 1u << 22;
-constexpr uint32_t kNodeOffset = (1u << 20) - 1u;
+// the join reads it), then decide the GMCR admission of every query graph
+// for the tile's 32 graphs (gmcr.hpp:33-128: every query vertex has a
+// candidate in the graph):
+//     admit[q][tile] = AND over q's classes c of NE(c),
+//     NE(c) = ballot over the tile's graphs of "AND of c's program planes != 0".
+// Warps take query graphs; a query's classes are visited in the order the
+// host chose (rarest label first, longer programs first), so most queries
+// are rejected for all 32 graphs after one or two classes and stop there.
+// NE(c) is computed at most once per tile per warp race (a shared-memory
+// cache with a valid bit per class), and a class's AND chain stops as soon as
+// it is zero in all 32 graphs.  The per-graph admitted counts (the GMCR
+// segment lengths) are summed in shared memory.  Queries of one vertex are
+// never admitted (the reference's mapping skips them, gmcr.hpp:100).
+constexpr uint32_t kAdmitWarps = 16;
 
 template <int AW>
-__global__ void __launch_bounds__(kWalkWarps * 32) k_planes_ne(
+__global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     uint32_t G, const uint32_t* __restrict__ goff, const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
     uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
-    int prof, const uint4* __restrict__ trie, uint32_t trie_n, const uint4* __restrict__ segs, uint32_t nsegs,
-    uint32_t nslots, uint64_t* __restrict__ planes, uint32_t* __restrict__ NE) {
-  extern __shared__ uint64_t tile[];  // [K * AW][32], then stacks [kWalkWarps][nslots][AW][32]
-  __shared__ uint32_t seg_next;
-  constexpr uint32_t kRow = AW * 32u;  // u64 words per plane row or stack slot
+    int prof, uint32_t QG, const uint32_t* __restrict__ qgoff, uint32_t C, const uint32_t* __restrict__ prog_off,
+    const uint16_t* __restrict__ prog, const uint32_t* __restrict__ qc_off, const uint32_t* __restrict__ qc,
+    uint64_t* __restrict__ planes, uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
+  extern __shared__ uint64_t tile[];  // [K * AW][32], then ne_word[C], ne_valid[(C + 31) / 32]
+  __shared__ uint32_t tile_cnt[32];
+  constexpr uint32_t kRow = AW * 32u;
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t GW = (G + 31u) / 32u;
-  const uint32_t words = K * AW;
-  const uint64_t* tl = tile + lane;  // tl[offset + 32 w]: word w of this lane's graph
-  uint64_t* sl = tile + static_cast<size_t>(words) * 32 + static_cast<size_t>(wid) * nslots * AW * 32 + lane;
-#pragma unroll
-  for (int w = 0; w < AW; ++w) sl[((nslots - 1) * AW + w) * 32] = ~0ull;  // the root slot
+  const uint32_t words = K * AW, CW = (C + 31u) / 32u;
+  uint32_t* ne_word = reinterpret_cast<uint32_t*>(tile + static_cast<size_t>(words) * 32);
+  uint32_t* ne_valid = ne_word + C;
+  const uint64_t* tl = tile + lane;
   for (uint32_t gw = blockIdx.x; gw < GW; gw += gridDim.x) {
     __syncthreads();  // the previous tile is no longer read
     for (uint32_t gl = wid; gl < 32; gl += nw) {
@@ -147,105 +133,125 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_planes_ne(
         for (uint32_t i = lane; i < words; i += 32) tile[i * 32 + gl] = 0;
       }
     }
-    if (threadIdx.x == 0) seg_next = 0;
+    for (uint32_t i = threadIdx.x; i < CW; i += blockDim.x) ne_valid[i] = 0;
+    if (threadIdx.x < 32) tile_cnt[threadIdx.x] = 0;
     __syncthreads();
     {
       uint4* dst = reinterpret_cast<uint4*>(planes + static_cast<uint64_t>(gw) * words * 32);
       const uint4* src = reinterpret_cast<const uint4*>(tile);
       for (uint32_t i = threadIdx.x; i < words * 16; i += blockDim.x) dst[i] = src[i];
     }
-    for (;;) {
-      uint32_t si = 0;
-      if (lane == 0) si = atomicAdd(&seg_next, 1u);
-      si = __shfl_sync(0xFFFFFFFFu, si, 0);
-      if (si >= nsegs) break;
-      const uint4 sg = segs[si];
-      uint64_t m[AW];
-#pragma unroll
-      for (int w = 0; w < AW; ++w) m[w] = ~0ull;
-      if (sg.z & 0x80000000u) {  // the segment starts below a top-level node: evaluate it
-#pragma unroll
-        for (int w = 0; w < AW; ++w) {
-          m[w] = tl[(sg.z & kNodeOffset) * kRow + 32 * w];
-          if (sg.z & kNodeBranch) sl[32 * w] = m[w];  // slot 0
-        }
-      }
-      uint32_t i = sg.x, wbase = 0xFFFFFFFFu;
-      uint4 win = make_uint4(0, 0, 0, 0);
-      while (i < sg.y) {
-        if (i < wbase || i - wbase >= 32u) {
-          wbase = i;
-          win = i + lane < trie_n ? trie[i + lane] : make_uint4(0, 0, 0, 0);
-        }
-        const uint32_t at = i - wbase;
-        const uint32_t x = __shfl_sync(0xFFFFFFFFu, win.x, at);
-        const uint32_t y = __shfl_sync(0xFFFFFFFFu, win.w, at);
-        const uint32_t off = (x & kNodeOffset) * kRow;
-        bool any = false;
-        if (x & kNodeStackRead) {
-#pragma unroll
-          for (int w = 0; w < AW; ++w) {
-            m[w] = sl[(y & 0xFFFFu) * kRow + 32 * w] & tl[off + 32 * w];
-            any |= m[w] != 0;
-          }
+    const uint32_t in_tile = G - gw * 32u;
+    const uint32_t valid_lanes = in_tile >= 32u ? 0xFFFFFFFFu : ((1u << in_tile) - 1u);
+    uint32_t my_cnt = 0;
+    for (uint32_t qg = wid; qg < QG; qg += nw) {
+      uint32_t alive = qgoff[qg + 1] - qgoff[qg] > 1u ? valid_lanes : 0u;
+      const uint32_t e1 = qc_off[qg + 1];
+      for (uint32_t e = qc_off[qg]; e < e1 && alive; ++e) {
+        const uint32_t c = qc[e];
+        uint32_t word;
+        if ((*reinterpret_cast<volatile uint32_t*>(&ne_valid[c >> 5]) >> (c & 31u)) & 1u) {
+          __threadfence_block();
+          word = *reinterpret_cast<volatile uint32_t*>(&ne_word[c]);
         } else {
+          uint64_t m[AW];
 #pragma unroll
-          for (int w = 0; w < AW; ++w) {
-            m[w] &= tl[off + 32 * w];
-            any |= m[w] != 0;
+          for (int w = 0; w < AW; ++w) m[w] = ~0ull;
+          bool any = true;
+          const uint32_t k1 = prog_off[c + 1];
+          for (uint32_t k = prog_off[c]; k < k1; ++k) {
+            const uint32_t off = static_cast<uint32_t>(prog[k]) * kRow;
+            any = false;
+#pragma unroll
+            for (int w = 0; w < AW; ++w) {
+              m[w] &= tl[off + 32 * w];
+              any |= m[w] != 0;
+            }
+            if (!__any_sync(0xFFFFFFFFu, any)) break;
+          }
+          word = __ballot_sync(0xFFFFFFFFu, any);
+          if (lane == 0) {
+            *reinterpret_cast<volatile uint32_t*>(&ne_word[c]) = word;
+            __threadfence_block();
+            atomicOr(&ne_valid[c >> 5], 1u << (c & 31u));
           }
         }
-        if (!__any_sync(0xFFFFFFFFu, any)) {
-          i = __shfl_sync(0xFFFFFFFFu, win.y, at);  // past this node's subtree
-          continue;
-        }
-        if (x & kNodeBranch) {
-#pragma unroll
-          for (int w = 0; w < AW; ++w) sl[(y >> 16) * kRow + 32 * w] = m[w];
-        }
-        if (x & kNodeTerminal) {
-          const uint32_t cls = __shfl_sync(0xFFFFFFFFu, win.z, at);
-          const uint32_t word = __ballot_sync(0xFFFFFFFFu, any);
-          if (lane == 0) NE[static_cast<uint64_t>(cls) * GW + gw] = word;
-        }
-        ++i;
+        alive &= word;
       }
+      if (lane == 0) admit[static_cast<uint64_t>(qg) * GW + gw] = alive;
+      my_cnt += (alive >> lane) & 1u;
     }
+    atomicAdd(&tile_cnt[lane], my_cnt);
+    __syncthreads();
+    if (threadIdx.x < 32 && gw * 32u + threadIdx.x < G) counts[gw * 32u + threadIdx.x] = tile_cnt[threadIdx.x];
   }
+}
+
+// Vertices per label value (shared-memory bins, one atomic per bin per block).
+__global__ void k_label_hist(const uint8_t* __restrict__ lab, uint64_t n, unsigned long long* __restrict__ hist) {
+  __shared__ unsigned int bins[256];
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) bins[i] = 0;
+  __syncthreads();
+  for (uint64_t v = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; v < n;
+       v += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    atomicAdd(&bins[lab[v]], 1u);
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x)
+    if (bins[i]) atomicAdd(&hist[i], static_cast<unsigned long long>(bins[i]));
 }
 
 }  // namespace
 
-size_t ne_planes_smem(uint32_t K, uint32_t AW, uint32_t nslots) {
-  return static_cast<size_t>(K) * AW * 32 * 8 + static_cast<size_t>(kWalkWarps) * nslots * AW * 32 * 8;
+int ensure_label_hist(Queue* q, Graph* g) {
+  if (g->label_hist.size() == 256) return SIGMO_OK;
+  void* buf = nullptr;
+  SIGMO_TRY(dev_alloc(q, &buf, 256 * 8));
+  int rc = SIGMO_OK;
+  if (cudaMemsetAsync(buf, 0, 256 * 8, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
+  if (!rc && g->total_nodes) {
+    k_label_hist<<<grid_for(g->total_nodes, 256, 148u * 4u), 256, 0, q->stream>>>(g->node_labels, g->total_nodes,
+                                                                                 static_cast<unsigned long long*>(buf));
+    rc = check_launch(q, "k_label_hist");
+  }
+  std::vector<uint64_t> h(256, 0);
+  if (!rc && (cudaMemcpyAsync(h.data(), buf, 256 * 8, cudaMemcpyDeviceToHost, q->stream) != cudaSuccess ||
+              cudaStreamSynchronize(q->stream) != cudaSuccess))
+    rc = fail(SIGMO_ERR_CUDA, "label histogram read-back failed");
+  dev_free(q, buf);
+  if (!rc) g->label_hist = std::move(h);
+  return rc;
 }
 
-int launch_planes_ne(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
-                     uint64_t* planes, uint32_t* NE) {
+size_t planes_admit_smem(uint32_t K, uint32_t AW, uint32_t C) {
+  return static_cast<size_t>(K) * AW * 32 * 8 + 4ull * C + 4ull * ((C + 31) / 32);
+}
+
+int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
+                        const PlaneProgram& pp, uint64_t* planes, uint32_t* admit, uint32_t* counts) {
   const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u;
   if (!GW) return SIGMO_OK;
-  SIGMO_CUDA_TRY(cudaMemsetAsync(NE, 0, 4ull * pp.C * GW, q->stream));
-  const size_t smem = ne_planes_smem(pp.K, data->adj_words, pp.nslots);
-  const unsigned block = 32u * kWalkWarps;
+  const size_t smem = planes_admit_smem(pp.K, data->adj_words, pp.C);
+  const unsigned block = 32u * kAdmitWarps;
   cudaError_t e = cudaSuccess;
   int per_sm = 0, sms = 0;
   SIGMO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device));
-#define SIGMO_PLANES_NE(AWV)                                                                                          \
-  e = cudaFuncSetAttribute(k_planes_ne<AWV>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));   \
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_planes_ne<AWV>, block, smem);    \
+#define SIGMO_PLANES_ADMIT(AWV)                                                                                       \
+  e = cudaFuncSetAttribute(k_planes_admit<AWV>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)); \
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_planes_admit<AWV>, block, smem); \
   if (e == cudaSuccess)                                                                                               \
-    k_planes_ne<AWV><<<std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms), block, smem,          \
-                       q->stream>>>(G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, pp.K,   \
-                                    pp.nlab, pp.spec, pp.r_begin, q->opts.profile, pp.trie, pp.trie_n, pp.segs,       \
-                                    pp.nsegs, pp.nslots, planes, NE)
+    k_planes_admit<AWV><<<std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms), block, smem,       \
+                          q->stream>>>(G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, pp.K, \
+                                       pp.nlab, pp.spec, pp.r_begin, q->opts.profile, query->num_graphs,              \
+                                       query->graph_offsets, pp.C, pp.prog_off, pp.prog, pp.qc_off, pp.qc, planes,     \
+                                       admit, counts)
   switch (data->adj_words) {
-    case 1: SIGMO_PLANES_NE(1); break;
-    case 2: SIGMO_PLANES_NE(2); break;
-    default: SIGMO_PLANES_NE(4); break;
+    case 1: SIGMO_PLANES_ADMIT(1); break;
+    case 2: SIGMO_PLANES_ADMIT(2); break;
+    default: SIGMO_PLANES_ADMIT(4); break;
   }
-#undef SIGMO_PLANES_NE
-  if (e != cudaSuccess) return fail(SIGMO_ERR_CUDA, "k_planes_ne shared-memory setup failed: %s", cudaGetErrorString(e));
-  return check_launch(q, "k_planes_ne");
+#undef SIGMO_PLANES_ADMIT
+  if (e != cudaSuccess) return fail(SIGMO_ERR_CUDA, "k_planes_admit shared-memory setup failed: %s", cudaGetErrorString(e));
+  return check_launch(q, "k_planes_admit");
 }
 
 }  // namespace sigmo_b200
