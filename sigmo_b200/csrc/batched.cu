@@ -242,11 +242,32 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   const uint64_t Wlow = L ? (static_cast<uint64_t>(data->host_graph_offsets[L]) + 31) / 32 : 0;
   const uint64_t Wlp = (Wlow + 31) / 32 * 32;
   auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-  const uint64_t b_dsig = run.dsig ? 0 : 8ull * R * N, b_planes = 8ull * GW * pp.K * AW * 32,
+  const ResidentPlanes* rp = run.resident;
+  const uint64_t b_dsig = run.dsig ? 0 : 8ull * R * N, b_planes = rp ? 0 : 8ull * GW * pp.K * AW * 32,
                  b_ne = 4ull * query->num_graphs * GW + 4ull * G;
+  // resident planes: the batch's plane k is resident row row_map[k], and the
+  // class programs are rewritten as resident rows for the join
+  std::vector<uint32_t> row_map;
+  std::vector<uint16_t> rprog;
+  if (rp) {
+    if (rp->R != R) return fail(SIGMO_ERR_INVALID, "resident planes hold %u iterations, the batch asks for %u", rp->R, R);
+    row_map.resize(pp.K);
+    for (uint32_t k = 0; k < pp.K; ++k) {
+      const uint32_t sp = pp.h_spec[k];
+      if (sp & 0x80000000u) {
+        row_map[k] = rp->label_row[sp & 0xFFu];
+      } else {
+        const uint32_t r = (sp >> 16) & 0xFFu, l = (sp >> 8) & 0xFFu, c = sp & 0xFFu;
+        row_map[k] = c <= rp->cmax[r * 16 + l] ? rp->base_row[r * 16 + l] + c - 1 : rp->zero_row;
+      }
+    }
+    rprog.resize(pp.h_prog.size());
+    for (size_t i = 0; i < rprog.size(); ++i) rprog[i] = static_cast<uint16_t>(row_map[pp.h_prog[i]]);
+  }
+  const uint64_t b_map = 4ull * row_map.size() + 2ull * rprog.size();
   const uint64_t b_lplanes = 16ull * 16 * R * Wlp, b_lbits = 4ull * Qn * Wlp;
   void* buf = nullptr;
-  SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + al(b_ne) + al(b_lplanes) + al(b_lbits) + 256));
+  SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + al(b_ne) + al(b_lplanes) + al(b_lbits) + al(b_map) + 256));
   char* p = static_cast<char*>(buf);
   uint64_t* dsig = run.dsig ? const_cast<uint64_t*>(run.dsig) : reinterpret_cast<uint64_t*>(p);
   p += al(b_dsig);
@@ -258,10 +279,20 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   uint32_t* lplanes = reinterpret_cast<uint32_t*>(p);
   p += al(b_lplanes);
   uint32_t* lbits = reinterpret_cast<uint32_t*>(p);
+  p += al(b_lbits);
+  uint32_t* d_row_map = reinterpret_cast<uint32_t*>(p);
+  uint16_t* d_rprog = reinterpret_cast<uint16_t*>(d_row_map + row_map.size());
   int rc = run.dsig ? SIGMO_OK : launch_sig_all(q, data, R, dsig);
+  if (!rc && rp) {
+    if (cudaMemcpyAsync(d_row_map, row_map.data(), 4ull * row_map.size(), cudaMemcpyHostToDevice, q->stream) != cudaSuccess ||
+        cudaMemcpyAsync(d_rprog, rprog.data(), 2ull * rprog.size(), cudaMemcpyHostToDevice, q->stream) != cudaSuccess)
+      rc = fail(SIGMO_ERR_CUDA, "H2D copy failed");
+  }
   if (!rc && cudaEventRecord(ev.e[1], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
   if (!rc) rc = order_classes(q, query, data);
-  if (!rc) rc = launch_planes_admit(q, query, data, dsig, R, pp, planes, admit, adm_counts);
+  if (!rc)
+    rc = rp ? launch_planes_admit_resident(q, query, data, *rp, pp, d_row_map, admit, adm_counts)
+            : launch_planes_admit(q, query, data, dsig, R, pp, planes, admit, adm_counts);
   if (!rc && cudaEventRecord(ev.e[2], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
   if (!rc) rc = launch_gmcr_from_admit(q, query, data, admit, adm_counts, m, true, 0);
   if (!rc && cudaEventRecord(ev.e[3], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
@@ -287,7 +318,9 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
     if (!rc) rc = join_literal_ranges(q, query, data, &view, m, find_first, L, d_total, run);
     q->stream = main_stream;
   }
-  if (!rc) rc = launch_join_fast_planes(q, query, data, pp, planes, m, find_first, d_total);
+  if (!rc)
+    rc = rp ? launch_join_fast_planes(q, query, data, pp, rp->planes, rp->rows, d_rprog, m, find_first, d_total)
+            : launch_join_fast_planes(q, query, data, pp, planes, pp.K, pp.prog, m, find_first, d_total);
   // join the side stream back before the scratch is released and the total read
   if (cudaEventRecord(q->ev_join, q->side) != cudaSuccess || cudaStreamWaitEvent(q->stream, q->ev_join, 0) != cudaSuccess)
     rc = rc ? rc : fail(SIGMO_ERR_CUDA, "stream join failed");

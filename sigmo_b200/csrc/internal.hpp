@@ -11,6 +11,8 @@
 
 namespace sigmo_b200 {
 
+struct ResidentPlanes;
+
 #define SIGMO_CUDA_TRY(expr)                                                                       \
   do {                                                                                             \
     cudaError_t _e = (expr);                                                                       \
@@ -165,12 +167,18 @@ int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const C
                         uint32_t graph_begin, uint32_t graph_end, uint64_t* d_total, uint32_t q_begin, uint32_t q_end);
 int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
                      uint64_t* d_total);
+// planes: [graph / 32][planes_rows][AW][32]; prog: the class programs as
+// row indices into it (pp.prog for the per-batch planes).
 int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, const PlaneProgram& pp, const uint64_t* planes,
-                            Gmcr* m, int find_first, uint64_t* d_total);
+                            uint32_t planes_rows, const uint16_t* prog, Gmcr* m, int find_first, uint64_t* d_total);
 int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const uint32_t* NE, const uint32_t* cls, Gmcr* m,
                         bool sync_total, uint64_t capacity_hint);
 int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
                         const PlaneProgram& pp, uint64_t* planes, uint32_t* admit, uint32_t* counts);
+// The same admission with the tile's planes gathered from resident planes
+// (row_map[k] = resident row of the batch's plane k).
+int launch_planes_admit_resident(Queue* q, const Graph* query, const Graph* data, const ResidentPlanes& rp,
+                                 const PlaneProgram& pp, const uint32_t* row_map, uint32_t* admit, uint32_t* counts);
 size_t planes_admit_smem(uint32_t K, uint32_t AW, uint32_t C);
 // GMCR from admission words admit[query graph][data graph / 32] and the
 // admitted count of every data graph (scan, total, sorted fill).
@@ -187,7 +195,22 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R);
 // data signatures already resident ([R][N], iterations 1..R), and the query
 // graph ranges of the requests batched together (nranges + 1 boundaries) so
 // the literal join of the low-offset graphs runs per request.
+// Planes of every threshold that occurs in a resident database (the serving
+// loop): rows [tile][rows][AW][32] u64; row `zero_row` is all zeros (a
+// threshold above every vertex's count, or a label that never occurs).
+struct ResidentPlanes {
+  uint64_t* planes = nullptr;
+  uint32_t rows = 0;
+  uint32_t zero_row = 0;
+  uint32_t R = 0;
+  std::vector<uint32_t> label_row;  // [256]
+  std::vector<uint32_t> base_row;   // [R][16]: row of (r, l, c = 1)
+  std::vector<uint8_t> cmax;        // [R][16]: largest count of label l at distance r+1 in any molecule
+};
+int build_resident_planes(Queue* q, Graph* data, const uint64_t* sig_all, uint32_t R, ResidentPlanes* out);
+
 struct BatchedRun {
+  const ResidentPlanes* resident = nullptr;
   const uint64_t* dsig = nullptr;
   const uint32_t* query_ranges = nullptr;
   uint32_t nranges = 0;

@@ -642,7 +642,7 @@ int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Cand
 }
 
 int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, const PlaneProgram& pp, const uint64_t* planes,
-                            Gmcr* m, int find_first, uint64_t* d_total) {
+                            uint32_t planes_rows, const uint16_t* prog, Gmcr* m, int find_first, uint64_t* d_total) {
   if (!m->total) return SIGMO_OK;
   if (query->max_nodes > kMaxQueryNodes)
     return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
@@ -674,7 +674,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
       auto* masks = static_cast<uint64_t*>(mbuf);
       auto* recs = reinterpret_cast<uint4*>(masks + kPhaseLevels * chunk);
       k_pair_masks<<<grid_for(cnt * kPhaseLevels, 256, 148u * 32u), 256, 0, q->stream>>>(
-          planes, pp.K, pp.prog_off, pp.prog, pp.cls, query->graph_offsets, query->qorder, query->sym, data->graph_offsets,
+          planes, planes_rows, pp.prog_off, prog, pp.cls, query->graph_offsets, query->qorder, query->sym, data->graph_offsets,
           data->sym, m->indices, m->pair_graph, slot0, cnt, masks, recs, skip, overflow, ctr + 2);
       rc = check_launch(q, "k_pair_masks");
       if (!rc && slot0 + chunk >= m->total && cudaEventRecord(q->ev_fork, q->stream) != cudaSuccess)
@@ -707,7 +707,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
     const uint32_t* list = tiles ? overflow : nullptr;
     const unsigned long long* list_len = tiles ? ctr + 2 : nullptr;
 #define SIGMO_JOIN_PLANES(AWV, EX)                                                                                      \
-  k_join_fast<AWV, EX, true><<<grid, block, 0, q->stream>>>(nullptr, 0, planes, pp.K, pp.prog_off, pp.prog, pp.cls,      \
+  k_join_fast<AWV, EX, true><<<grid, block, 0, q->stream>>>(nullptr, 0, planes, planes_rows, pp.prog_off, prog, pp.cls,  \
                                                             q->opts.profile, query->graph_offsets, query->qorder,        \
                                                             query->qsel, query->qsel_id, query->sym, data->graph_offsets, \
                                                             data->adj, data->sym, m->indices, m->pair_graph, list,       \

@@ -107,13 +107,43 @@ __device__ __forceinline__ void build_graph_planes(uint64_t* tile, uint32_t gl, 
 // never admitted (the reference's mapping skips them, gmcr.hpp:100).
 constexpr uint32_t kAdmitWarps = 16;
 
-template <int AW>
+// The tile's planes: built from the data signatures (and written out for the
+// join), or gathered from resident planes (rows row_map[k] of the tile).
+template <int AW, bool GATHER>
+__device__ __forceinline__ void fill_tile(uint64_t* tile, uint32_t gw, uint32_t G, const uint32_t* __restrict__ goff,
+                                          const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all, uint64_t N,
+                                          uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec,
+                                          const uint32_t* __restrict__ r_begin, int prof, const uint64_t* __restrict__ rplanes,
+                                          uint32_t rrows, const uint32_t* __restrict__ row_map) {
+  constexpr uint32_t kRow = AW * 32u;
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (GATHER) {
+    const uint64_t* src = rplanes + static_cast<uint64_t>(gw) * rrows * kRow;
+    for (uint32_t k = wid; k < K; k += nw) {
+      const uint64_t* row = src + static_cast<uint64_t>(row_map[k]) * kRow;
+#pragma unroll
+      for (int w = 0; w < AW; ++w) tile[k * kRow + 32 * w + lane] = row[32 * w + lane];
+    }
+  } else {
+    for (uint32_t gl = wid; gl < 32; gl += nw) {
+      const uint32_t g = gw * 32u + gl;
+      if (g < G) {
+        build_graph_planes<AW>(tile, gl, goff[g], goff[g + 1], lane, lab, sig_all, N, R, nlab, spec, r_begin, prof);
+      } else {
+        for (uint32_t i = lane; i < K * AW; i += 32) tile[i * 32 + gl] = 0;
+      }
+    }
+  }
+}
+
+template <int AW, bool GATHER>
 __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     uint32_t G, const uint32_t* __restrict__ goff, const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
     uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
-    int prof, uint32_t QG, const uint32_t* __restrict__ qgoff, uint32_t C, const uint32_t* __restrict__ prog_off,
-    const uint16_t* __restrict__ prog, const uint32_t* __restrict__ qc_off, const uint32_t* __restrict__ qc,
-    uint64_t* __restrict__ planes, uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
+    int prof, const uint64_t* __restrict__ rplanes, uint32_t rrows, const uint32_t* __restrict__ row_map, uint32_t QG,
+    const uint32_t* __restrict__ qgoff, uint32_t C, const uint32_t* __restrict__ prog_off, const uint16_t* __restrict__ prog,
+    const uint32_t* __restrict__ qc_off, const uint32_t* __restrict__ qc, uint64_t* __restrict__ planes,
+    uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
   extern __shared__ uint64_t tile[];  // [K * AW][32], then ne_word[C], ne_valid[(C + 31) / 32]
   __shared__ uint32_t tile_cnt[32];
   constexpr uint32_t kRow = AW * 32u;
@@ -125,18 +155,11 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
   const uint64_t* tl = tile + lane;
   for (uint32_t gw = blockIdx.x; gw < GW; gw += gridDim.x) {
     __syncthreads();  // the previous tile is no longer read
-    for (uint32_t gl = wid; gl < 32; gl += nw) {
-      const uint32_t g = gw * 32u + gl;
-      if (g < G) {
-        build_graph_planes<AW>(tile, gl, goff[g], goff[g + 1], lane, lab, sig_all, N, R, nlab, spec, r_begin, prof);
-      } else {
-        for (uint32_t i = lane; i < words; i += 32) tile[i * 32 + gl] = 0;
-      }
-    }
+    fill_tile<AW, GATHER>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, rplanes, rrows, row_map);
     for (uint32_t i = threadIdx.x; i < CW; i += blockDim.x) ne_valid[i] = 0;
     if (threadIdx.x < 32) tile_cnt[threadIdx.x] = 0;
     __syncthreads();
-    {
+    if (!GATHER) {
       uint4* dst = reinterpret_cast<uint4*>(planes + static_cast<uint64_t>(gw) * words * 32);
       const uint4* src = reinterpret_cast<const uint4*>(tile);
       for (uint32_t i = threadIdx.x; i < words * 16; i += blockDim.x) dst[i] = src[i];
@@ -187,6 +210,46 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
   }
 }
 
+// Planes of a fixed spec for every graph, into out[tile][out_rows][AW][32]
+// (rows K .. out_rows - 1 zeroed): the resident planes of the serving loop.
+template <int AW>
+__global__ void __launch_bounds__(kAdmitWarps * 32) k_build_planes(
+    uint32_t G, const uint32_t* __restrict__ goff, const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
+    uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
+    int prof, uint32_t out_rows, uint64_t* __restrict__ out) {
+  extern __shared__ uint64_t tile[];  // [K * AW][32]
+  const uint32_t GW = (G + 31u) / 32u;
+  for (uint32_t gw = blockIdx.x; gw < GW; gw += gridDim.x) {
+    __syncthreads();
+    fill_tile<AW, false>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, nullptr, 0, nullptr);
+    __syncthreads();
+    uint4* dst = reinterpret_cast<uint4*>(out + static_cast<uint64_t>(gw) * out_rows * AW * 32);
+    const uint4* src = reinterpret_cast<const uint4*>(tile);
+    const uint32_t have = K * AW * 16, all = out_rows * AW * 16;
+    for (uint32_t i = threadIdx.x; i < all; i += blockDim.x) dst[i] = i < have ? src[i] : make_uint4(0, 0, 0, 0);
+  }
+}
+
+// Largest count of label l at iteration r over all vertices: cmax[r * 16 + l].
+__global__ void k_sig_cmax(const uint64_t* __restrict__ sig_all, uint64_t N, uint32_t R, unsigned int* __restrict__ cmax) {
+  for (uint32_t r = 0; r < R; ++r) {
+    uint32_t mx[16];
+#pragma unroll
+    for (int l = 0; l < 16; ++l) mx[l] = 0;
+    for (uint64_t v = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; v < N;
+         v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+      const uint64_t sv = sig_all[static_cast<uint64_t>(r) * N + v];
+#pragma unroll
+      for (int l = 0; l < 16; ++l) mx[l] = max(mx[l], static_cast<uint32_t>((sv >> (4 * l)) & 0xFull));
+    }
+#pragma unroll
+    for (int l = 0; l < 16; ++l) {
+      const uint32_t m = __reduce_max_sync(0xFFFFFFFFu, mx[l]);
+      if ((threadIdx.x & 31u) == 0 && m) atomicMax(&cmax[r * 16 + l], m);
+    }
+  }
+}
+
 // Vertices per label value (shared-memory bins, one atomic per bin per block).
 __global__ void k_label_hist(const uint8_t* __restrict__ lab, uint64_t n, unsigned long long* __restrict__ hist) {
   __shared__ unsigned int bins[256];
@@ -226,32 +289,136 @@ size_t planes_admit_smem(uint32_t K, uint32_t AW, uint32_t C) {
   return static_cast<size_t>(K) * AW * 32 * 8 + 4ull * C + 4ull * ((C + 31) / 32);
 }
 
-int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
-                        const PlaneProgram& pp, uint64_t* planes, uint32_t* admit, uint32_t* counts) {
+namespace {
+
+template <int AW, bool GATHER>
+int admit_launch(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
+                 const uint64_t* rplanes, uint32_t rrows, const uint32_t* row_map, uint64_t* planes, uint32_t* admit,
+                 uint32_t* counts) {
   const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u;
-  if (!GW) return SIGMO_OK;
-  const size_t smem = planes_admit_smem(pp.K, data->adj_words, pp.C);
+  const size_t smem = planes_admit_smem(pp.K, AW, pp.C);
   const unsigned block = 32u * kAdmitWarps;
-  cudaError_t e = cudaSuccess;
   int per_sm = 0, sms = 0;
   SIGMO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device));
-#define SIGMO_PLANES_ADMIT(AWV)                                                                                       \
-  e = cudaFuncSetAttribute(k_planes_admit<AWV>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)); \
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_planes_admit<AWV>, block, smem); \
-  if (e == cudaSuccess)                                                                                               \
-    k_planes_admit<AWV><<<std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms), block, smem,       \
-                          q->stream>>>(G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, pp.K, \
-                                       pp.nlab, pp.spec, pp.r_begin, q->opts.profile, query->num_graphs,              \
-                                       query->graph_offsets, pp.C, pp.prog_off, pp.prog, pp.qc_off, pp.qc, planes,     \
-                                       admit, counts)
-  switch (data->adj_words) {
-    case 1: SIGMO_PLANES_ADMIT(1); break;
-    case 2: SIGMO_PLANES_ADMIT(2); break;
-    default: SIGMO_PLANES_ADMIT(4); break;
-  }
-#undef SIGMO_PLANES_ADMIT
+  cudaError_t e = cudaFuncSetAttribute(k_planes_admit<AW, GATHER>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_planes_admit<AW, GATHER>, block, smem);
   if (e != cudaSuccess) return fail(SIGMO_ERR_CUDA, "k_planes_admit shared-memory setup failed: %s", cudaGetErrorString(e));
+  const uint64_t grid = std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms);
+  k_planes_admit<AW, GATHER><<<grid, block, smem, q->stream>>>(
+      G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, pp.K, pp.nlab, pp.spec, pp.r_begin,
+      q->opts.profile, rplanes, rrows, row_map, query->num_graphs, query->graph_offsets, pp.C, pp.prog_off, pp.prog, pp.qc_off,
+      pp.qc, planes, admit, counts);
   return check_launch(q, "k_planes_admit");
+}
+
+}  // namespace
+
+int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
+                        const PlaneProgram& pp, uint64_t* planes, uint32_t* admit, uint32_t* counts) {
+  if (!data->num_graphs) return SIGMO_OK;
+  switch (data->adj_words) {
+    case 1: return admit_launch<1, false>(q, query, data, sig_all, R, pp, nullptr, 0, nullptr, planes, admit, counts);
+    case 2: return admit_launch<2, false>(q, query, data, sig_all, R, pp, nullptr, 0, nullptr, planes, admit, counts);
+    default: return admit_launch<4, false>(q, query, data, sig_all, R, pp, nullptr, 0, nullptr, planes, admit, counts);
+  }
+}
+
+int launch_planes_admit_resident(Queue* q, const Graph* query, const Graph* data, const ResidentPlanes& rp,
+                                 const PlaneProgram& pp, const uint32_t* row_map, uint32_t* admit, uint32_t* counts) {
+  if (!data->num_graphs) return SIGMO_OK;
+  switch (data->adj_words) {
+    case 1: return admit_launch<1, true>(q, query, data, nullptr, 0, pp, rp.planes, rp.rows, row_map, nullptr, admit, counts);
+    case 2: return admit_launch<2, true>(q, query, data, nullptr, 0, pp, rp.planes, rp.rows, row_map, nullptr, admit, counts);
+    default: return admit_launch<4, true>(q, query, data, nullptr, 0, pp, rp.planes, rp.rows, row_map, nullptr, admit, counts);
+  }
+}
+
+// Resident planes of every (label) and (iteration, label, count) that occurs
+// in the database: label planes for each label present and the wildcard,
+// thresholds c = 1..cmax(r, l), then one zero row.
+int build_resident_planes(Queue* q, Graph* data, const uint64_t* sig_all, uint32_t R, ResidentPlanes* out) {
+  SIGMO_TRY(ensure_label_hist(q, data));
+  const uint64_t N = data->total_nodes;
+  const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, AW = data->adj_words;
+  std::vector<unsigned int> cmax(16ull * (R ? R : 1), 0);
+  if (R && N) {
+    void* d = nullptr;
+    SIGMO_TRY(dev_alloc(q, &d, 4ull * 16 * R));
+    int rc = cudaMemsetAsync(d, 0, 4ull * 16 * R, q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "memset failed");
+    if (!rc) {
+      k_sig_cmax<<<grid_for(N, 256, 148u * 8u), 256, 0, q->stream>>>(sig_all, N, R, static_cast<unsigned int*>(d));
+      rc = check_launch(q, "k_sig_cmax");
+    }
+    if (!rc && (cudaMemcpyAsync(cmax.data(), d, 4ull * 16 * R, cudaMemcpyDeviceToHost, q->stream) != cudaSuccess ||
+                cudaStreamSynchronize(q->stream) != cudaSuccess))
+      rc = fail(SIGMO_ERR_CUDA, "cmax read-back failed");
+    dev_free(q, d);
+    SIGMO_TRY(rc);
+  }
+  std::vector<uint32_t> spec;
+  out->label_row.assign(256, 0);
+  for (uint32_t l = 0; l < 256; ++l)
+    if (data->label_hist[l] || l == kWildcard) {
+      out->label_row[l] = static_cast<uint32_t>(spec.size());
+      spec.push_back(0x80000000u | l);
+    }
+  const uint32_t nlab = static_cast<uint32_t>(spec.size());
+  std::vector<uint32_t> r_begin(R + 1, 0);
+  out->base_row.assign(16ull * R, 0);
+  out->cmax.assign(16ull * R, 0);
+  for (uint32_t r = 0; r < R; ++r) {
+    r_begin[r] = static_cast<uint32_t>(spec.size());
+    for (uint32_t l = 0; l < 16; ++l) {
+      const uint32_t cm = cmax[r * 16 + l];
+      out->cmax[r * 16 + l] = static_cast<uint8_t>(cm);
+      out->base_row[r * 16 + l] = static_cast<uint32_t>(spec.size());
+      for (uint32_t c = 1; c <= cm; ++c) spec.push_back((r << 16) | (l << 8) | c);
+    }
+  }
+  r_begin[R] = static_cast<uint32_t>(spec.size());
+  const uint32_t K = static_cast<uint32_t>(spec.size());
+  out->zero_row = K;
+  for (uint32_t l = 0; l < 256; ++l)
+    if (!data->label_hist[l] && l != kWildcard) out->label_row[l] = K;
+  out->rows = K + 1;
+  out->R = R;
+  const size_t smem = static_cast<size_t>(K) * AW * 32 * 8;
+  if (smem > 200u * 1024u) return fail(SIGMO_ERR_DOMAIN, "the database needs %u resident planes (too many for one tile)", K);
+  void* dspec = nullptr;
+  void* drb = nullptr;
+  SIGMO_TRY(dev_alloc(q, &dspec, 4ull * K));
+  SIGMO_TRY(dev_alloc(q, &drb, 4ull * (R + 1)));
+  int rc = SIGMO_OK;
+  if (cudaMemcpyAsync(dspec, spec.data(), 4ull * K, cudaMemcpyHostToDevice, q->stream) != cudaSuccess ||
+      cudaMemcpyAsync(drb, r_begin.data(), 4ull * (R + 1), cudaMemcpyHostToDevice, q->stream) != cudaSuccess)
+    rc = fail(SIGMO_ERR_CUDA, "H2D copy failed");
+  if (!rc) rc = dev_alloc(q, reinterpret_cast<void**>(&out->planes), 8ull * GW * out->rows * AW * 32 + 8);
+  if (!rc && GW) {
+    int per_sm = 0, sms = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device);
+    const unsigned block = 32u * kAdmitWarps;
+#define SIGMO_BUILD(AWV)                                                                                             \
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_build_planes<AWV>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                                 static_cast<int>(smem));                                            \
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_planes<AWV>, block, smem);  \
+  if (e == cudaSuccess)                                                                                              \
+    k_build_planes<AWV><<<std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms), block, smem,      \
+                          q->stream>>>(G, data->graph_offsets, data->node_labels, sig_all, N, R, K, nlab,            \
+                                       static_cast<const uint32_t*>(dspec), static_cast<const uint32_t*>(drb),        \
+                                       q->opts.profile, out->rows, out->planes)
+    switch (AW) {
+      case 1: SIGMO_BUILD(1); break;
+      case 2: SIGMO_BUILD(2); break;
+      default: SIGMO_BUILD(4); break;
+    }
+#undef SIGMO_BUILD
+    if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "k_build_planes setup failed: %s", cudaGetErrorString(e));
+    if (!rc) rc = check_launch(q, "k_build_planes");
+  }
+  if (!rc && cudaStreamSynchronize(q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "resident plane build failed");
+  dev_free(q, dspec);
+  dev_free(q, drb);
+  return rc;
 }
 
 }  // namespace sigmo_b200

@@ -125,6 +125,7 @@ struct Server {
   sigmo_queue_t q0 = nullptr;
   sigmo_graph_t data = nullptr;
   uint64_t* dsig = nullptr;
+  ResidentPlanes rp;  // every threshold plane of the database
   uint64_t resident_bytes = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done, cv_mem;
@@ -143,14 +144,15 @@ struct Server {
 
 namespace {
 
-// Device footprint of a batch once its plane program is known: planes, the
+// Device footprint of a batch once its plane program is known: planes (none
+// when the database's planes are resident), the
 // non-empty matrix, the GMCR arrays for every (query, data graph) pair, the
 // join's per-chunk level masks and the result arrays.
-uint64_t projected_bytes(const Graph* query, const Graph* data) {
+uint64_t projected_bytes(const Graph* query, const Graph* data, bool resident) {
   const PlaneProgram& pp = query->pp;
   const uint64_t G = data->num_graphs, GW = (G + 31) / 32, QG = query->num_graphs;
   const uint64_t pairs = QG * G;
-  const uint64_t planes = 8ull * GW * 32 * pp.K * data->adj_words;
+  const uint64_t planes = resident ? 0 : 8ull * GW * 32 * pp.K * data->adj_words;
   const uint64_t ne = 4ull * pp.C * GW + 4ull * QG * GW;
   const uint64_t gmcr = 4ull * (G + 1) + pairs * (4 + 4 + 8);
   const uint64_t join = std::min<uint64_t>(pairs, 8ull << 20) * (8ull * 16 + 16) + 4ull * pairs;
@@ -253,7 +255,7 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
   if (!rc) note(build_plane_program(q, qg, so.iterations));
   // admission by the batch's projected device footprint
   if (!rc) {
-    const uint64_t need = projected_bytes(qg, data);
+    const uint64_t need = projected_bytes(qg, data, rp.planes != nullptr);
     std::unique_lock<std::mutex> lk(mu);
     if (need > so.memory_budget) {
       note(fail(SIGMO_ERR_OOM, "batch of %llu query graphs needs %llu bytes, above the serving memory budget (%llu bytes)",
@@ -271,6 +273,7 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
   if (!rc) {
     BatchedRun run;
     run.dsig = dsig;
+    run.resident = rp.planes ? &rp : nullptr;
     run.query_ranges = ranges.data();
     run.nranges = static_cast<uint32_t>(batch.size());
     note(match_batched(q, qg, data, so.iterations, so.find_first, false, nullptr, w->m, &mr, run));
@@ -482,6 +485,7 @@ int sigmo_server_create(int device, const sigmo_host_graphs* database, const sig
   SIGMO_TRY(sigmo_queue_create(device, opts, &s->q0));
   s->opts = s->q0->opts;
   auto cleanup = [&](int rc) {
+    if (s->rp.planes) dev_free(s->q0, s->rp.planes);
     if (s->dsig) dev_free(s->q0, s->dsig);
     if (s->data) sigmo_graph_destroy(s->data);
     cudaStreamSynchronize(s->q0->stream);
@@ -497,9 +501,20 @@ int sigmo_server_create(int device, const sigmo_host_graphs* database, const sig
   rc = dev_alloc(s->q0, reinterpret_cast<void**>(&s->dsig), 8ull * (o.iterations ? o.iterations : 1) * (N ? N : 1));
   if (!rc && o.iterations) rc = launch_sig_all(s->q0, s->data, o.iterations, s->dsig);
   if (!rc && cudaStreamSynchronize(s->q0->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "database upload failed");
+  // the planes of every threshold that occurs in the database, built once:
+  // a batch then gathers its planes instead of evaluating signatures
+  if (!rc && o.iterations) {
+    rc = build_resident_planes(s->q0, s->data, s->dsig, o.iterations, &s->rp);
+    if (rc == SIGMO_ERR_DOMAIN) {  // too many distinct thresholds for one tile: build planes per batch
+      if (s->rp.planes) dev_free(s->q0, s->rp.planes);
+      s->rp = ResidentPlanes{};
+      rc = SIGMO_OK;
+    }
+  }
   if (rc) return cleanup(rc);
   s->resident_bytes = 4ull * (s->data->num_graphs + 1) + 4ull * (N + 1) + 5ull * s->data->total_edges + N +
-                      4ull * N + 8ull * N * s->data->adj_words + 8ull * o.iterations * N;
+                      4ull * N + 8ull * N * s->data->adj_words + 8ull * o.iterations * N +
+                      8ull * ((s->data->num_graphs + 31) / 32) * 32 * s->rp.rows * s->data->adj_words;
   if (o.memory_budget == 0) {
     size_t freeb = 0, totalb = 0;
     if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) return cleanup(fail(SIGMO_ERR_CUDA, "cudaMemGetInfo failed"));
@@ -624,6 +639,7 @@ int sigmo_server_destroy(sigmo_server_t s) {
       sigmo_queue_destroy(w.q);
     }
   }
+  if (s->rp.planes) dev_free(s->q0, s->rp.planes);
   if (s->dsig) dev_free(s->q0, s->dsig);
   if (s->data) sigmo_graph_destroy(s->data);
   cudaStreamSynchronize(s->q0->stream);
