@@ -250,8 +250,8 @@ def run_serving(args, d, wl, local):
     import sigmo_b200 as sb
 
     if args.serve_mols and args.serve_mols != d.num_graphs:
-        d = sb.generate_molecules(args.serve_mols, wl["min_atoms"], wl["max_atoms"], seed=wl["seed_d"] + 17, kind=wl["kind"],
-                                  median=wl["median"])
+        # the serving database shape: molecules of 10-40 heavy atoms (5M molecules ~ 125M vertices)
+        d = sb.generate_molecules(args.serve_mols, 10, 40, seed=wl["seed_d"] + 17, kind=0)
     rng = np.random.default_rng(4242)
     n_req = max(1, int(round(args.serve_rate * args.serve_seconds)))
     sizes = rng.integers(1, 65, n_req)
@@ -261,10 +261,12 @@ def run_serving(args, d, wl, local):
     srv = sb.Server(d, device=local, iterations=wl["R"], find_first=True, max_inflight=args.serve_inflight,
                     max_batch_queries=64)
     setup_s = time.perf_counter() - t_setup
-    # warm-up: a few requests before the timed arrivals
-    for t in [srv.submit(reqs[i % n_req]) for i in range(4)]:
-        srv.wait(t)
-        srv.release(t)
+    # warm-up: requests before the timed arrivals, some at once so that every
+    # worker has run (and the memory pool holds) concurrent batches
+    for rounds in range(2):
+        for t in [srv.submit(reqs[i % n_req]) for i in range(2 * args.serve_inflight)]:
+            srv.wait(t)
+            srv.release(t)
     tickets = [None] * n_req
 
     def submitter():

@@ -298,8 +298,11 @@ typedef struct sigmo_request_result {
   uint32_t batch_requests;
   uint64_t projected_bytes;    /* the batch's admitted device footprint                        */
   double ms_queue;             /* submit -> batch start (host clock)                           */
-  double ms_device;            /* the batch's device time (CUDA events)                        */
+  double ms_device;            /* the batch's stream time, upload to results (CUDA events)     */
   double ms_latency;           /* submit -> results on the host (host clock)                   */
+  double ms_filter;            /* the batch's stages (CUDA events; sigmo_match_result)         */
+  double ms_mapping;
+  double ms_join;
 } sigmo_request_result;
 
 typedef struct sigmo_server_stats {

@@ -69,6 +69,9 @@ class RequestResultC(ctypes.Structure):
         ("ms_queue", ctypes.c_double),
         ("ms_device", ctypes.c_double),
         ("ms_latency", ctypes.c_double),
+        ("ms_filter", ctypes.c_double),
+        ("ms_mapping", ctypes.c_double),
+        ("ms_join", ctypes.c_double),
     ]
 
 

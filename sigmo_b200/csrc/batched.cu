@@ -167,6 +167,7 @@ int order_classes(Queue* q, Graph* query, Graph* data) {
   SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
   pp.qc_for = data;
   pp.qc_stamp = data->stamp;
+  pp.h_qc_n = list.size();
   return SIGMO_OK;
 }
 

@@ -64,6 +64,7 @@ struct PlaneProgram {
   // graph's label frequencies (rebuilt when the data graph changes)
   uint32_t* qc_off = nullptr;     // [query graphs + 1]
   uint32_t* qc = nullptr;
+  size_t h_qc_n = 0;              // entries of qc
   const void* qc_for = nullptr;   // the data graph the order was built for
   uint64_t qc_stamp = 0;
   uint64_t* qsig_all = nullptr;   // [R][query vertices] signatures, iterations 1..R

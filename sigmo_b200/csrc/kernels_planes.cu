@@ -136,26 +136,105 @@ __device__ __forceinline__ void fill_tile(uint64_t* tile, uint32_t gw, uint32_t 
   }
 }
 
+// 16-byte asynchronous global -> shared copies (no registers in between).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Resident rows row_map[k] of tile gw into dst (K rows of AW x 32 words),
+// as 16-byte asynchronous copies spread over the block.
+template <int AW>
+__device__ __forceinline__ void gather_tile_async(uint64_t* dst, const uint64_t* __restrict__ rplanes, uint32_t rrows,
+                                                  uint32_t gw, uint32_t K, const uint32_t* s_map) {
+  constexpr uint32_t kRow = AW * 32u, kChunks = AW * 16u;  // 16-byte chunks per row
+  const uint64_t* src = rplanes + static_cast<uint64_t>(gw) * rrows * kRow;
+  for (uint32_t i = threadIdx.x; i < K * kChunks; i += blockDim.x) {
+    const uint32_t k = i / kChunks, c = i % kChunks;
+    cp_async16(dst + k * kRow + 2 * c, src + static_cast<uint64_t>(s_map[k]) * kRow + 2 * c);
+  }
+  cp_async_commit();
+}
+
+// Shared-memory layout of k_planes_admit (in u64 units for the tiles):
+//   tile buffer(s) [1 or 2][K * AW * 32] u64, ne_word[C], ne_valid[CW],
+//   s_map[K] (gather), then the staged class lists when they fit:
+//   qc_off[QG + 1], qc[n_qc], prog_off[C + 1] (u32), prog[n_prog] (u16).
+struct AdmitSmem {
+  size_t tiles, ne_word, ne_valid, map, lists, total;
+};
+__host__ __device__ inline AdmitSmem admit_smem_layout(uint32_t K, uint32_t AW, uint32_t C, bool gather, size_t list_bytes) {
+  AdmitSmem l{};
+  l.tiles = 0;
+  size_t off = static_cast<size_t>(gather ? 2 : 1) * K * AW * 32 * 8;
+  l.ne_word = off;
+  off += 4ull * C;
+  l.ne_valid = off;
+  off += 4ull * ((C + 31) / 32);
+  l.map = off;
+  off += gather ? 4ull * K : 0;
+  off = (off + 15) & ~static_cast<size_t>(15);
+  l.lists = off;
+  off += list_bytes;
+  l.total = off;
+  return l;
+}
+
 template <int AW, bool GATHER>
 __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     uint32_t G, const uint32_t* __restrict__ goff, const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
     uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
     int prof, const uint64_t* __restrict__ rplanes, uint32_t rrows, const uint32_t* __restrict__ row_map, uint32_t QG,
-    const uint32_t* __restrict__ qgoff, uint32_t C, const uint32_t* __restrict__ prog_off, const uint16_t* __restrict__ prog,
-    const uint32_t* __restrict__ qc_off, const uint32_t* __restrict__ qc, uint64_t* __restrict__ planes,
-    uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
-  extern __shared__ uint64_t tile[];  // [K * AW][32], then ne_word[C], ne_valid[(C + 31) / 32]
+    const uint32_t* __restrict__ qgoff, uint32_t C, const uint32_t* __restrict__ g_prog_off, const uint16_t* __restrict__ g_prog,
+    const uint32_t* __restrict__ g_qc_off, const uint32_t* __restrict__ g_qc, uint32_t n_qc, uint32_t n_prog, int stage_lists,
+    uint64_t* __restrict__ planes, uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t tile_cnt[32];
   constexpr uint32_t kRow = AW * 32u;
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t GW = (G + 31u) / 32u;
   const uint32_t words = K * AW, CW = (C + 31u) / 32u;
-  uint32_t* ne_word = reinterpret_cast<uint32_t*>(tile + static_cast<size_t>(words) * 32);
-  uint32_t* ne_valid = ne_word + C;
-  const uint64_t* tl = tile + lane;
+  const size_t list_bytes = stage_lists ? 4ull * (QG + 1 + n_qc + C + 1) + 2ull * n_prog : 0;
+  const AdmitSmem L = admit_smem_layout(K, AW, C, GATHER, list_bytes);
+  uint64_t* tiles = reinterpret_cast<uint64_t*>(smem_raw);
+  uint32_t* ne_word = reinterpret_cast<uint32_t*>(smem_raw + L.ne_word);
+  uint32_t* ne_valid = reinterpret_cast<uint32_t*>(smem_raw + L.ne_valid);
+  uint32_t* s_map = reinterpret_cast<uint32_t*>(smem_raw + L.map);
+  // per-batch constants: the row map and (when they fit) the class lists
+  const uint32_t* qc_off = g_qc_off;
+  const uint32_t* qc = g_qc;
+  const uint32_t* prog_off = g_prog_off;
+  const uint16_t* prog = g_prog;
+  if (GATHER)
+    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) s_map[i] = row_map[i];
+  if (stage_lists) {
+    uint32_t* p = reinterpret_cast<uint32_t*>(smem_raw + L.lists);
+    for (uint32_t i = threadIdx.x; i <= QG; i += blockDim.x) p[i] = g_qc_off[i];
+    for (uint32_t i = threadIdx.x; i < n_qc; i += blockDim.x) p[QG + 1 + i] = g_qc[i];
+    for (uint32_t i = threadIdx.x; i <= C; i += blockDim.x) p[QG + 1 + n_qc + i] = g_prog_off[i];
+    uint16_t* p16 = reinterpret_cast<uint16_t*>(p + QG + 1 + n_qc + C + 1);
+    for (uint32_t i = threadIdx.x; i < n_prog; i += blockDim.x) p16[i] = g_prog[i];
+    qc_off = p;
+    qc = p + QG + 1;
+    prog_off = p + QG + 1 + n_qc;
+    prog = p16;
+  }
+  __syncthreads();
+  uint32_t buf = 0;
+  if (GATHER && blockIdx.x < GW) gather_tile_async<AW>(tiles, rplanes, rrows, blockIdx.x, K, s_map);
   for (uint32_t gw = blockIdx.x; gw < GW; gw += gridDim.x) {
-    __syncthreads();  // the previous tile is no longer read
-    fill_tile<AW, GATHER>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, rplanes, rrows, row_map);
+    uint64_t* tile = tiles + static_cast<size_t>(buf) * words * 32;
+    if (GATHER) {
+      cp_async_wait_all();
+      __syncthreads();  // this tile has landed; every warp is done with the previous one
+      const uint32_t next = gw + gridDim.x;
+      if (next < GW) gather_tile_async<AW>(tiles + static_cast<size_t>(buf ^ 1u) * words * 32, rplanes, rrows, next, K, s_map);
+    } else {
+      __syncthreads();  // the previous tile is no longer read
+      fill_tile<AW, false>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, nullptr, 0, nullptr);
+    }
     for (uint32_t i = threadIdx.x; i < CW; i += blockDim.x) ne_valid[i] = 0;
     if (threadIdx.x < 32) tile_cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -164,6 +243,7 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
       const uint4* src = reinterpret_cast<const uint4*>(tile);
       for (uint32_t i = threadIdx.x; i < words * 16; i += blockDim.x) dst[i] = src[i];
     }
+    const uint64_t* tl = tile + lane;
     const uint32_t in_tile = G - gw * 32u;
     const uint32_t valid_lanes = in_tile >= 32u ? 0xFFFFFFFFu : ((1u << in_tile) - 1u);
     uint32_t my_cnt = 0;
@@ -207,7 +287,9 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     atomicAdd(&tile_cnt[lane], my_cnt);
     __syncthreads();
     if (threadIdx.x < 32 && gw * 32u + threadIdx.x < G) counts[gw * 32u + threadIdx.x] = tile_cnt[threadIdx.x];
+    buf ^= GATHER ? 1u : 0u;
   }
+  if (GATHER) cp_async_wait_all();
 }
 
 // Planes of a fixed spec for every graph, into out[tile][out_rows][AW][32]
@@ -286,7 +368,7 @@ int ensure_label_hist(Queue* q, Graph* g) {
 }
 
 size_t planes_admit_smem(uint32_t K, uint32_t AW, uint32_t C) {
-  return static_cast<size_t>(K) * AW * 32 * 8 + 4ull * C + 4ull * ((C + 31) / 32);
+  return admit_smem_layout(K, AW, C, false, 0).total;
 }
 
 namespace {
@@ -295,8 +377,14 @@ template <int AW, bool GATHER>
 int admit_launch(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
                  const uint64_t* rplanes, uint32_t rrows, const uint32_t* row_map, uint64_t* planes, uint32_t* admit,
                  uint32_t* counts) {
-  const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u;
-  const size_t smem = planes_admit_smem(pp.K, AW, pp.C);
+  const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, QG = query->num_graphs;
+  const uint32_t n_qc = static_cast<uint32_t>(pp.h_qc_n), n_prog = static_cast<uint32_t>(pp.h_prog.size());
+  const size_t list_bytes = 4ull * (QG + 1 + n_qc + pp.C + 1) + 2ull * n_prog;
+  const size_t base = admit_smem_layout(pp.K, AW, pp.C, GATHER, 0).total;
+  // stage the class lists when the block still fits three to an SM
+  const int stage = base + list_bytes <= 72u * 1024u ? 1 : 0;
+  const size_t smem = admit_smem_layout(pp.K, AW, pp.C, GATHER, stage ? list_bytes : 0).total;
+  if (smem > 220u * 1024u) return fail(SIGMO_ERR_DOMAIN, "k_planes_admit needs %zu bytes of shared memory", smem);
   const unsigned block = 32u * kAdmitWarps;
   int per_sm = 0, sms = 0;
   SIGMO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device));
@@ -306,8 +394,8 @@ int admit_launch(Queue* q, const Graph* query, const Graph* data, const uint64_t
   const uint64_t grid = std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms);
   k_planes_admit<AW, GATHER><<<grid, block, smem, q->stream>>>(
       G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, pp.K, pp.nlab, pp.spec, pp.r_begin,
-      q->opts.profile, rplanes, rrows, row_map, query->num_graphs, query->graph_offsets, pp.C, pp.prog_off, pp.prog, pp.qc_off,
-      pp.qc, planes, admit, counts);
+      q->opts.profile, rplanes, rrows, row_map, QG, query->graph_offsets, pp.C, pp.prog_off, pp.prog, pp.qc_off, pp.qc, n_qc,
+      n_prog, stage, planes, admit, counts);
   return check_launch(q, "k_planes_admit");
 }
 

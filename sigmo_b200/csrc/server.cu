@@ -378,6 +378,9 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
       o.ms_queue = ms_between(r->t_submit, r->t_start);
       o.ms_device = dev_ms;
       o.ms_latency = ms_between(r->t_submit, t_done);
+      o.ms_filter = mr.ms_signatures + mr.ms_filter;
+      o.ms_mapping = mr.ms_mapping;
+      o.ms_join = mr.ms_join;
       o.projected_bytes = reserved;
       o.pairs = static_cast<uint64_t>(r->num_queries) * data->num_graphs;
       if (!rc) {
