@@ -1,0 +1,61 @@
+"""The bench's multi-rank plumbing on CPU: two gloo ranks, each with its own
+replica of the workload (weak scaling, no data-path collective), the timing
+reduced as the max over ranks and the per-rank results checked against the
+same replicas computed in one process.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import bench
+
+WL = dict(desc="tiny", mols=40, min_atoms=8, max_atoms=20, kind=0, median=14.0, queries=6, qmin=3, qmax=7, skew=(0, 0),
+          qkind=0, R=2, seed_d=77, seed_q=78)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    import torch
+
+    import oracle
+
+    dist = bench.init_dist(world, "gloo")
+    q, d = bench.make_workload(WL, rank)
+    res = oracle.run_pipeline(q, d, WL["R"], oracle.REF_PTX, False)
+    # each rank reports its own device-style time; the bench keeps the max
+    mx = bench.max_over_ranks(dist, float(10 + rank), device=None)
+    tot = torch.tensor([res["total"]], dtype=torch.float64)
+    dist.all_reduce(tot)
+    out[rank] = (int(res["total"]), int(d.graph_offsets[-1]), mx, float(tot.item()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_two_gloo_ranks_run_independent_replicas():
+    world = 2
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
+        got = dict(out)
+    import oracle
+
+    want = []
+    for r in range(world):
+        q, d = bench.make_workload(WL, r)
+        want.append((int(oracle.run_pipeline(q, d, WL["R"], oracle.REF_PTX, False)["total"]), int(d.graph_offsets[-1])))
+    assert got[0][0] == want[0][0] and got[1][0] == want[1][0]
+    assert got[0][1] != got[1][1] or got[0][0] != got[1][0], "ranks were given the same replica"
+    assert got[0][2] == got[1][2] == 11.0  # max over ranks
+    assert got[0][3] == got[1][3] == float(want[0][0] + want[1][0])
+    assert np.isfinite(got[0][3])
