@@ -72,6 +72,8 @@ def parse_args():
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean request arrivals per second (Poisson)")
     ap.add_argument("--serve-mols", type=int, default=0, help="serving database size (0: the workload's molecules)")
     ap.add_argument("--serve-inflight", type=int, default=2)
+    ap.add_argument("--no-graph", action="store_true", help="time ordinary calls instead of CUDA-graph replays")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default join launch shape")
     return ap.parse_args()
 
 
@@ -332,12 +334,25 @@ def run_sigmo(args, rank, world, local):
     gm = sb.GMCR(queue)
     stream = torch.cuda.ExternalStream(queue.stream, device=local)
 
+    tuning = None
+    if not args.no_autotune:
+        tuning = sb.autotune(queue, qg, dg, R, ff, reps=2)
+    graph = not args.no_graph
     for _ in range(max(args.warmup, 0)):
         res = sb.match_batched(queue, qg, dg, R, ff, None, gm)
     queue.wait()
 
+    # ---- per-stage device times: ordinary calls (CUDA events per stage) ----
+    stage = []
+    for _ in range(args.steps):
+        stage.append(sb.match_batched(queue, qg, dg, R, ff, None, gm))
+    if graph:  # capture, then warm the replay
+        for _ in range(max(args.warmup, 1)):
+            sb.match_batched(queue, qg, dg, R, ff, None, gm, graph=True)
+    queue.wait()
+
     # ---- timed region: K steps, device-resident inputs ----
-    step_ms, stage = [], []
+    step_ms = []
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -347,9 +362,8 @@ def run_sigmo(args, rank, world, local):
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         for _ in range(args.steps):
-            res = sb.match_batched(queue, qg, dg, R, ff, None, gm)
+            res = sb.match_batched(queue, qg, dg, R, ff, None, gm, graph=graph)
             step_ms.append(res["ms_total"])
-            stage.append(res)
         ev1.record(stream)
         ev1.synchronize()
         torch.cuda.synchronize()
@@ -529,6 +543,8 @@ def run_sigmo(args, rank, world, local):
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
+        "cuda_graph": graph,
+        "tuning": tuning,
         "serving": serving,
     }
     print(json.dumps(out))

@@ -110,6 +110,17 @@ typedef struct sigmo_options {
 } sigmo_options;
 
 SIGMO_API void sigmo_default_options(sigmo_options* o);
+
+/* Launch shape of the batched join (no reference counterpart; the
+ * reference's only knob is the join work-group size above).  Zero fields take
+ * the defaults.  sigmo_autotune searches these on a caller's own workload. */
+typedef struct sigmo_tuning {
+  uint32_t join_blocks_per_sm;   /* persistent join CTAs per SM, 1..3 (3)                      */
+  uint32_t join_chunk;           /* GMCR slots a lane takes per work grab, 1..64 (4)             */
+  uint32_t overflow_blocks;      /* CTAs of the join for queries over 16 vertices (1184)        */
+  uint32_t overflow_serial;      /* 1: run those after the main join instead of beside it (0)   */
+  uint32_t mask_chunk_slots;     /* GMCR slots per level-mask pass, in 2^20 units, 1..64 (8)     */
+} sigmo_tuning;
 /* sycl::queue{gpu_selector_v, enable_profiling} (library/src/sigmo.cpp:19). */
 SIGMO_API int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out);
 SIGMO_API int sigmo_queue_destroy(sigmo_queue_t q);
@@ -117,6 +128,9 @@ SIGMO_API int sigmo_queue_destroy(sigmo_queue_t q);
 SIGMO_API int sigmo_queue_wait(sigmo_queue_t q);
 /* The queue's cudaStream_t (as void*), for callers that order work with it. */
 SIGMO_API int sigmo_queue_stream(sigmo_queue_t q, void** stream);
+/* The join launch shape used by this queue (defaults until set). */
+SIGMO_API int sigmo_queue_set_tuning(sigmo_queue_t q, const sigmo_tuning* t);
+SIGMO_API int sigmo_queue_get_tuning(sigmo_queue_t q, sigmo_tuning* t);
 /* BatchedEvent::getProfilingInfo (library/include/utils.hpp:149-157): device
  * time of the last stage launched on the queue, after it has completed. */
 SIGMO_API int sigmo_queue_last_stage_ms(sigmo_queue_t q, double* ms);
@@ -244,7 +258,16 @@ SIGMO_API int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_
  * synchronisation.  The final candidate bitset is not written unless
  * SIGMO_MATCH_MATERIALIZE_BITSET is given (then `c` receives it); `c` may be
  * NULL otherwise.  GMCR and per-pair counts stay on the device in `m`. */
-enum { SIGMO_MATCH_MATERIALIZE_BITSET = 1 };
+enum { SIGMO_MATCH_MATERIALIZE_BITSET = 1,
+       /* Graph mode (no reference counterpart): the first call with these
+        * graphs runs normally and then captures the batch's device work into
+        * a CUDA graph kept on `m`; later calls with the same query and data
+        * graphs, iterations, mode, profile and tuning replay it (one launch,
+        * one host synchronisation).  A replay whose admitted total differs
+        * from the captured one (the graphs' device arrays were changed) runs
+        * and captures again.  Stage times other than ms_total are 0 on a
+        * replay. */
+       SIGMO_MATCH_CUDA_GRAPH = 2 };
 
 typedef struct sigmo_match_result {
   uint64_t total_matches;     /* sum over admitted pairs                     */
@@ -259,6 +282,13 @@ typedef struct sigmo_match_result {
 
 SIGMO_API int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t iterations,
                         int find_first, uint32_t flags, sigmo_candidates_t c, sigmo_gmcr_t m, sigmo_match_result* out);
+/* Autotuner (no reference counterpart): runs sigmo_match_batched on these
+ * graphs under candidate join launch shapes (coordinate descent over the
+ * sigmo_tuning fields, `reps` timed runs per candidate, median join time),
+ * keeps the fastest on the queue and returns it.  Every candidate must give
+ * the same total as the default shape, or the call fails. */
+SIGMO_API int sigmo_autotune(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t iterations, int find_first,
+                             uint32_t reps, sigmo_tuning* best, double* best_ms, double* default_ms);
 /* Per-pair counts of the last sigmo_match_batched call on `m` (GMCR slot order). */
 SIGMO_API int sigmo_match_download_counts(sigmo_gmcr_t m, uint64_t* per_pair, uint64_t len);
 

@@ -210,6 +210,19 @@ class Queue:
         check(lib().sigmo_queue_stream(self._h, ctypes.byref(p)))
         return p.value or 0
 
+    def set_tuning(self, **fields):
+        """Join launch shape (sigmo_tuning); unspecified fields keep their value."""
+        t = _L.TuningC()
+        check(lib().sigmo_queue_get_tuning(self._h, ctypes.byref(t)))
+        for k, v in fields.items():
+            setattr(t, k, int(v))
+        check(lib().sigmo_queue_set_tuning(self._h, ctypes.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = _L.TuningC()
+        check(lib().sigmo_queue_get_tuning(self._h, ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in _L.TuningC._fields_}
+
     def launch_count(self) -> int:
         v = ctypes.c_uint64()
         check(lib().sigmo_queue_launch_count(self._h, ctypes.byref(v)))
@@ -463,18 +476,35 @@ def joinCandidates(queue: Queue, query_graphs, data_graphs, candidates: Candidat
 MATCH_MATERIALIZE_BITSET = 1
 
 
+MATCH_CUDA_GRAPH = 2
+
+
 def match_batched(queue: Queue, query_graphs, data_graphs, iterations: int, find_first: bool,
-                  candidates: Candidates | None, gmcr: GMCR, materialize: bool = False) -> dict:
+                  candidates: Candidates | None, gmcr: GMCR, materialize: bool = False, graph: bool = False) -> dict:
     """The batched form: signatures for all iterations, candidate planes,
     GMCR and the persistent join in one call (same GMCR and counts as the
     stage calls).  With materialize=True the final candidate bitset is also
-    written into `candidates`."""
+    written into `candidates`.  With graph=True the batch is captured into a
+    CUDA graph on the first call and replayed by later calls with the same
+    graphs (SIGMO_MATCH_CUDA_GRAPH)."""
     res = _L.MatchResultC()
-    flags = MATCH_MATERIALIZE_BITSET if materialize else 0
+    flags = (MATCH_MATERIALIZE_BITSET if materialize else 0) | (MATCH_CUDA_GRAPH if graph else 0)
     check(lib().sigmo_match_batched(queue._h, query_graphs._h, data_graphs._h, iterations, int(bool(find_first)), flags,
                                     candidates._h if candidates is not None else None, gmcr._h, ctypes.byref(res)))
     gmcr._num_data_graphs = data_graphs.num_graphs
     return {f: getattr(res, f) for f, _ in _L.MatchResultC._fields_}
+
+
+def autotune(queue: Queue, query_graphs, data_graphs, iterations: int, find_first: bool, reps: int = 3) -> dict:
+    """Searches the join launch shape on these graphs (sigmo_autotune), keeps
+    the fastest on the queue and returns it with the median join times."""
+    t = _L.TuningC()
+    best, default = ctypes.c_double(), ctypes.c_double()
+    check(lib().sigmo_autotune(queue._h, query_graphs._h, data_graphs._h, iterations, int(bool(find_first)), reps,
+                               ctypes.byref(t), ctypes.byref(best), ctypes.byref(default)))
+    out = {f: getattr(t, f) for f, _ in _L.TuningC._fields_}
+    out.update(ms_join=best.value, ms_join_default=default.value)
+    return out
 
 
 # ---- serving loop -----------------------------------------------------------------

@@ -44,6 +44,16 @@ class MatchResultC(ctypes.Structure):
     ]
 
 
+class TuningC(ctypes.Structure):
+    _fields_ = [
+        ("join_blocks_per_sm", ctypes.c_uint32),
+        ("join_chunk", ctypes.c_uint32),
+        ("overflow_blocks", ctypes.c_uint32),
+        ("overflow_serial", ctypes.c_uint32),
+        ("mask_chunk_slots", ctypes.c_uint32),
+    ]
+
+
 class ServerOptionsC(ctypes.Structure):
     _fields_ = [
         ("iterations", ctypes.c_uint32),
@@ -143,6 +153,9 @@ SIGNATURES = {
     "sigmo_gmcr_generate_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _u64, _P(_u64)]),
     "sigmo_join_candidates": (_i, [_vp, _vp, _vp, _vp, _vp, _P(_u64), _i, _vp]),
     "sigmo_match_batched": (_i, [_vp, _vp, _vp, _u32, _i, _u32, _vp, _vp, _P(MatchResultC)]),
+    "sigmo_queue_set_tuning": (_i, [_vp, _P(TuningC)]),
+    "sigmo_queue_get_tuning": (_i, [_vp, _P(TuningC)]),
+    "sigmo_autotune": (_i, [_vp, _vp, _vp, _u32, _i, _u32, _P(TuningC), _P(_d), _P(_d)]),
     "sigmo_server_default_options": (None, [_P(ServerOptionsC)]),
     "sigmo_server_create": (_i, [_i, _P(HostGraphsC), _vp, _P(ServerOptionsC), _P(_vp)]),
     "sigmo_server_submit": (_i, [_vp, _P(HostGraphsC), _u32, _P(_u64)]),

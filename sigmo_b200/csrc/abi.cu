@@ -13,6 +13,20 @@
 
 namespace sigmo_b200 {
 
+int normalize_tuning(sigmo_tuning* t) {
+  const sigmo_tuning d{3, 4, 148 * 8, 0, 8};
+  if (!t->join_blocks_per_sm) t->join_blocks_per_sm = d.join_blocks_per_sm;
+  if (!t->join_chunk) t->join_chunk = d.join_chunk;
+  if (!t->overflow_blocks) t->overflow_blocks = d.overflow_blocks;
+  if (!t->mask_chunk_slots) t->mask_chunk_slots = d.mask_chunk_slots;
+  if (t->join_blocks_per_sm > 3) return fail(SIGMO_ERR_INVALID, "join_blocks_per_sm must be 1..3");
+  if (t->join_chunk > 64) return fail(SIGMO_ERR_INVALID, "join_chunk must be 1..64");
+  if (t->overflow_blocks > 65535) return fail(SIGMO_ERR_INVALID, "overflow_blocks must be <= 65535");
+  if (t->overflow_serial > 1) return fail(SIGMO_ERR_INVALID, "overflow_serial must be 0 or 1");
+  if (t->mask_chunk_slots > 64) return fail(SIGMO_ERR_INVALID, "mask_chunk_slots must be 1..64");
+  return SIGMO_OK;
+}
+
 int check_launch(Queue* q, const char* what) {
   q->launches++;
   cudaError_t e = cudaGetLastError();
@@ -195,6 +209,20 @@ int sigmo_queue_device_info(sigmo_queue_t q, uint64_t* global_mem, char* name, s
     std::strncpy(name, p.name, name_len - 1);
     name[name_len - 1] = 0;
   }
+  return SIGMO_OK;
+}
+
+int sigmo_queue_set_tuning(sigmo_queue_t q, const sigmo_tuning* t) {
+  if (!q || !t) return fail(SIGMO_ERR_INVALID, "null argument");
+  sigmo_tuning n = *t;
+  SIGMO_TRY(normalize_tuning(&n));
+  q->tune = n;
+  return SIGMO_OK;
+}
+
+int sigmo_queue_get_tuning(sigmo_queue_t q, sigmo_tuning* t) {
+  if (!q || !t) return fail(SIGMO_ERR_INVALID, "null argument");
+  *t = q->tune;
   return SIGMO_OK;
 }
 
@@ -558,6 +586,7 @@ int sigmo_gmcr_create(sigmo_queue_t q, sigmo_gmcr_t* out) {
 int sigmo_gmcr_destroy(sigmo_gmcr_t m) {
   if (!m) return SIGMO_OK;
   cudaSetDevice(m->q->device);
+  if (m->graph) cudaGraphExecDestroy(m->graph);
   dev_free(m->q, m->offsets);
   dev_free(m->q, m->indices);
   dev_free(m->q, m->pair_graph);
@@ -568,6 +597,11 @@ int sigmo_gmcr_destroy(sigmo_gmcr_t m) {
 
 int sigmo_gmcr_generate(sigmo_gmcr_t m, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c) {
   if (!m || !query || !data || !c) return fail(SIGMO_ERR_INVALID, "null argument");
+  if (m->graph) {  // the captured batch refers to the arrays this call may replace
+    cudaGraphExecDestroy(m->graph);
+    m->graph = nullptr;
+    for (auto& k : m->graph_key) k = 0;
+  }
   if (c->rows != query->total_nodes || c->targets != data->total_nodes)
     return fail(SIGMO_ERR_INVALID, "candidate bitset does not match the graphs");
   Queue* q = m->q;

@@ -234,6 +234,11 @@ int batched_bitset(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
 // The plane route (no full bitset in HBM).
 int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, Gmcr* m, uint64_t* d_total, Events& ev,
                    const BatchedRun& run) {
+  // stage events are not recorded while the work is captured into a graph
+  auto mark = [&](int i) -> int {
+    if (run.capture) return SIGMO_OK;
+    return cudaEventRecord(ev.e[i], q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "event record failed");
+  };
   PlaneProgram& pp = query->pp;
   const uint64_t N = data->total_nodes, Qn = query->total_nodes;
   const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, AW = data->adj_words;
@@ -289,14 +294,16 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
         cudaMemcpyAsync(d_rprog, rprog.data(), 2ull * rprog.size(), cudaMemcpyHostToDevice, q->stream) != cudaSuccess)
       rc = fail(SIGMO_ERR_CUDA, "H2D copy failed");
   }
-  if (!rc && cudaEventRecord(ev.e[1], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc) rc = mark(1);
   if (!rc) rc = order_classes(q, query, data);
   if (!rc)
     rc = rp ? launch_planes_admit_resident(q, query, data, *rp, pp, d_row_map, admit, adm_counts)
             : launch_planes_admit(q, query, data, dsig, R, pp, planes, admit, adm_counts);
-  if (!rc && cudaEventRecord(ev.e[2], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
-  if (!rc) rc = launch_gmcr_from_admit(q, query, data, admit, adm_counts, m, true, 0);
-  if (!rc && cudaEventRecord(ev.e[3], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc) rc = mark(2);
+  // captured: the admitted total of the run that built the graph sizes the
+  // arrays (the replay checks that it did not change)
+  if (!rc) rc = launch_gmcr_from_admit(q, query, data, admit, adm_counts, m, !run.capture, run.capture ? m->total : 0);
+  if (!rc) rc = mark(3);
   const bool literal = !rc && L && m->total;
   if (literal) {
     // REF_PTX: graphs starting below vertex 256 keep the reference's live
@@ -333,14 +340,103 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
 
 namespace sigmo_b200 {
 
+namespace {
+
+void drop_graph(Gmcr* m) {
+  if (m->graph) cudaGraphExecDestroy(m->graph);
+  m->graph = nullptr;
+  for (auto& k : m->graph_key) k = 0;
+}
+
+// Replays the captured batch: the device work of the planes route (no host
+// synchronisation inside), then the match total and the GMCR total to the
+// queue's pinned buffer.  Returns SIGMO_ERR_INVALID (and drops the graph)
+// when the admitted total differs from the one the graph was sized for.
+int replay_graph(Queue* q, Graph* query, Graph* data, Gmcr* m, sigmo_match_result* out) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  SIGMO_CUDA_TRY(cudaEventCreate(&e0));
+  SIGMO_CUDA_TRY(cudaEventCreate(&e1));
+  cudaError_t e = cudaEventRecord(e0, q->stream);
+  if (e == cudaSuccess) e = cudaGraphLaunch(m->graph, q->stream);
+  if (e == cudaSuccess) q->launches += m->graph_launches;
+  if (e == cudaSuccess) e = cudaEventRecord(e1, q->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(q->stream);
+  float f = 0;
+  if (e == cudaSuccess) cudaEventElapsedTime(&f, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return fail(SIGMO_ERR_CUDA, "graph replay failed: %s", cudaGetErrorString(e));
+  const uint64_t* pin = static_cast<const uint64_t*>(q->pinned);
+  const uint32_t gtotal = *reinterpret_cast<const uint32_t*>(pin + 1);
+  if (gtotal != m->total) {
+    drop_graph(m);
+    return fail(SIGMO_ERR_INVALID, "the admitted total changed since the graph was captured");
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->total_matches = pin[0];
+  out->admitted_pairs = m->total;
+  out->pairs = static_cast<uint64_t>(query->num_graphs) * data->num_graphs;
+  out->ms_total = f;
+  m->counts_valid = true;
+  return SIGMO_OK;
+}
+
+// Captures the planes route for (query, data) into m->graph, sized by the
+// admitted total of the run that just completed.
+int capture_graph(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, Gmcr* m, const BatchedRun& run0) {
+  drop_graph(m);
+  BatchedRun run = run0;
+  run.capture = true;
+  Events ev;  // unused while capturing
+  const uint64_t launches0 = q->launches;
+  SIGMO_CUDA_TRY(cudaStreamBeginCapture(q->stream, cudaStreamCaptureModeThreadLocal));
+  uint64_t* d_total = nullptr;
+  int rc = dev_alloc(q, reinterpret_cast<void**>(&d_total), 8);
+  if (!rc && cudaMemsetAsync(d_total, 0, 8, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
+  if (!rc) rc = batched_planes(q, query, data, R, find_first, m, d_total, ev, run);
+  uint64_t* pin = static_cast<uint64_t*>(q->pinned);
+  if (!rc && (cudaMemcpyAsync(pin, d_total, 8, cudaMemcpyDeviceToHost, q->stream) != cudaSuccess ||
+              cudaMemcpyAsync(pin + 1, m->offsets + data->num_graphs, 4, cudaMemcpyDeviceToHost, q->stream) != cudaSuccess))
+    rc = fail(SIGMO_ERR_CUDA, "capture of the read-back failed");
+  if (d_total) dev_free(q, d_total);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(q->stream, &g);
+  if (!rc && ec != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(ec));
+  if (!rc) {
+    const cudaError_t ei = cudaGraphInstantiate(&m->graph, g, 0);
+    if (ei != cudaSuccess) {
+      m->graph = nullptr;
+      rc = fail(SIGMO_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ei));
+    }
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  m->graph_launches = q->launches - launches0;
+  q->launches = launches0;  // nothing ran during the capture
+  m->counts_valid = true;   // the counts of the run before the capture are still in place
+  return rc;
+}
+
+}  // namespace
+
 int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, bool materialize, Candidates* c, Gmcr* m,
-                  sigmo_match_result* out, const BatchedRun& run) {
+                  sigmo_match_result* out, const BatchedRun& run, bool graph) {
   if (query->max_nodes > kMaxQueryNodes)
     return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
   if (data->max_nodes > 64u * kMaxAdjWords)
     return fail(SIGMO_ERR_DOMAIN, "the batched form supports data graphs of up to %u vertices (largest: %u)", 64u * kMaxAdjWords,
                 data->max_nodes);
   SIGMO_CUDA_TRY(cudaSetDevice(q->device));
+  const sigmo_tuning& tn = q->tune;
+  const uint64_t key[6] = {query->stamp, data->stamp, R, static_cast<uint64_t>(find_first),
+                           static_cast<uint64_t>(q->opts.profile) | (static_cast<uint64_t>(tn.overflow_serial) << 8),
+                           (static_cast<uint64_t>(tn.join_blocks_per_sm) << 48) | (static_cast<uint64_t>(tn.join_chunk) << 40) |
+                               (static_cast<uint64_t>(tn.mask_chunk_slots) << 32) | tn.overflow_blocks};
+  if (graph && !materialize && m->graph && std::equal(key, key + 6, m->graph_key)) {
+    const int rc = replay_graph(q, query, data, m, out);
+    if (rc != SIGMO_ERR_INVALID) return rc;  // else: recapture below
+  }
+  drop_graph(m);  // this run may replace the arrays a captured batch refers to
   std::memset(out, 0, sizeof(*out));
   Events ev;
   for (auto& e : ev.e) SIGMO_CUDA_TRY(cudaEventCreate(&e));
@@ -350,8 +446,9 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
   int rc = cudaMemsetAsync(d_total, 0, 8, q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "memset failed");
   const bool planes_fit = planes_admit_smem(query->pp.K, data->adj_words, query->pp.C) <= 200u * 1024u;
+  const bool bitset_route = materialize || !planes_fit;
   if (!rc) {
-    if (materialize || !planes_fit) {
+    if (bitset_route) {
       sigmo_candidates_t cc = static_cast<sigmo_candidates_t>(c);
       if (!cc) rc = sigmo_candidates_create(static_cast<sigmo_queue_t>(q), query->total_nodes, data->total_nodes, &cc);
       if (!rc) rc = batched_bitset(q, query, data, R, find_first, cc, m, d_total, ev, run);
@@ -384,6 +481,11 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
     m->counts_valid = true;
   }
   dev_free(q, d_total);
+  if (!rc && graph && !bitset_route) {
+    // graph mode: capture this batch for the next calls with the same inputs
+    rc = capture_graph(q, query, data, R, find_first, m, run);
+    if (!rc) std::copy(key, key + 6, m->graph_key);
+  }
   return rc;
 }
 
@@ -397,5 +499,74 @@ extern "C" int sigmo_match_batched(sigmo_queue_t q, sigmo_graph_t query, sigmo_g
   if (c && (c->rows != query->total_nodes || c->targets != data->total_nodes))
     return fail(SIGMO_ERR_INVALID, "candidate bitset does not match the graphs");
   if (m->q != q || (c && c->q != q) || query->q != q || data->q != q) return fail(SIGMO_ERR_INVALID, "handles belong to another queue");
-  return match_batched(q, query, data, R, find_first, materialize, c, m, out, BatchedRun{});
+  return match_batched(q, query, data, R, find_first, materialize, c, m, out, BatchedRun{},
+                       (flags & SIGMO_MATCH_CUDA_GRAPH) != 0);
+}
+
+// ---- autotuner --------------------------------------------------------------
+extern "C" int sigmo_autotune(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, uint32_t R, int find_first,
+                              uint32_t reps, sigmo_tuning* best, double* best_ms, double* default_ms) {
+  if (!q || !query || !data || !best) return fail(SIGMO_ERR_INVALID, "null argument");
+  if (query->q != q || data->q != q) return fail(SIGMO_ERR_INVALID, "handles belong to another queue");
+  if (reps == 0) reps = 3;
+  sigmo_gmcr_t m = nullptr;
+  SIGMO_TRY(sigmo_gmcr_create(q, &m));
+  const sigmo_tuning saved = q->tune;
+  auto measure = [&](const sigmo_tuning& t, double* ms, uint64_t* total) -> int {
+    q->tune = t;
+    std::vector<double> js;
+    sigmo_match_result r{};
+    for (uint32_t i = 0; i <= reps; ++i) {
+      SIGMO_TRY(match_batched(q, query, data, R, find_first, false, nullptr, m, &r, BatchedRun{}));
+      if (i) js.push_back(r.ms_join);
+    }
+    std::sort(js.begin(), js.end());
+    *ms = js[js.size() / 2];
+    *total = r.total_matches;
+    return SIGMO_OK;
+  };
+  sigmo_tuning cur{};
+  normalize_tuning(&cur);
+  double cur_ms = 0, d_ms = 0;
+  uint64_t d_total = 0, total = 0;
+  int rc = measure(cur, &d_ms, &d_total);
+  cur_ms = d_ms;
+  struct Axis {
+    uint32_t sigmo_tuning::*field;
+    std::vector<uint32_t> values;
+  };
+  const Axis axes[] = {
+      {&sigmo_tuning::overflow_serial, {0, 1}},
+      {&sigmo_tuning::join_blocks_per_sm, {1, 2, 3}},
+      {&sigmo_tuning::join_chunk, {1, 2, 4, 8, 16}},
+      {&sigmo_tuning::overflow_blocks, {148, 296, 592, 1184, 2368}},
+      {&sigmo_tuning::mask_chunk_slots, {2, 8, 32}},
+  };
+  for (const Axis& ax : axes) {
+    for (uint32_t v : ax.values) {
+      if (rc) break;
+      if (cur.*ax.field == v) continue;
+      sigmo_tuning t = cur;
+      t.*ax.field = v;
+      double ms = 0;
+      rc = measure(t, &ms, &total);
+      if (!rc && total != d_total)
+        rc = fail(SIGMO_ERR_INVALID, "autotune: a launch shape changed the result (%llu vs %llu)", (unsigned long long)total,
+                  (unsigned long long)d_total);
+      if (!rc && ms < cur_ms * 0.98) {
+        cur = t;
+        cur_ms = ms;
+      }
+    }
+  }
+  sigmo_gmcr_destroy(m);
+  if (rc) {
+    q->tune = saved;
+    return rc;
+  }
+  q->tune = cur;
+  *best = cur;
+  if (best_ms) *best_ms = cur_ms;
+  if (default_ms) *default_ms = d_ms;
+  return SIGMO_OK;
 }

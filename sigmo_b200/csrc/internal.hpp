@@ -32,6 +32,7 @@ struct Queue {
   int device = 0;
   cudaStream_t stream = nullptr;
   sigmo_options opts{};
+  sigmo_tuning tune{3, 4, 148 * 8, 0, 8};
   cudaEvent_t ev_start = nullptr, ev_end = nullptr;
   bool stage_recorded = false;
   uint64_t launches = 0;
@@ -130,6 +131,10 @@ struct Gmcr {
   uint64_t total = 0;
   uint64_t capacity = 0;
   bool counts_valid = false;
+  // CUDA graph of the last batched match run in graph mode, and what it was built for
+  cudaGraphExec_t graph = nullptr;
+  uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+  uint64_t graph_launches = 0;  // kernels in the captured batch
 };
 
 // Stage timing: every public stage brackets its launches with these.
@@ -191,6 +196,8 @@ int launch_fused_filter_raw(Queue* q, const uint8_t* qlab, const uint64_t* qsig_
                             uint64_t N, const uint32_t* planes_all, uint64_t Wstride, uint32_t R, uint32_t* bits);
 int launch_row_counts(Queue* q, const Candidates* c, uint32_t* d_counts);
 int build_plane_program(Queue* q, Graph* query, uint32_t R);
+// Fills zero fields of a tuning with the defaults and checks the ranges.
+int normalize_tuning(sigmo_tuning* t);
 
 // Options of the batched form beyond the C entry point (the serving loop):
 // data signatures already resident ([R][N], iterations 1..R), and the query
@@ -211,13 +218,14 @@ struct ResidentPlanes {
 int build_resident_planes(Queue* q, Graph* data, const uint64_t* sig_all, uint32_t R, ResidentPlanes* out);
 
 struct BatchedRun {
+  bool capture = false;  // the work is being captured into a CUDA graph: no host synchronisation
   const ResidentPlanes* resident = nullptr;
   const uint64_t* dsig = nullptr;
   const uint32_t* query_ranges = nullptr;
   uint32_t nranges = 0;
 };
 int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_first, bool materialize, Candidates* c, Gmcr* m,
-                  sigmo_match_result* out, const BatchedRun& run);
+                  sigmo_match_result* out, const BatchedRun& run, bool graph = false);
 void release_plane_program(Graph* g);
 int launch_digest(Queue* q, const Candidates* c, uint64_t* d_digest);
 

@@ -500,9 +500,8 @@ template <bool EXACT>
 __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
     const uint64_t* __restrict__ masks, const uint4* __restrict__ rec, uint64_t slot0, uint64_t count,
     const uint64_t* __restrict__ qsel, const uint64_t* __restrict__ qsel_id, const uint64_t* __restrict__ dadj,
-    uint32_t skip_below, int find_first, unsigned long long* __restrict__ cursor, uint64_t* __restrict__ counts,
-    unsigned long long* __restrict__ d_total) {
-  constexpr uint32_t kChunk = 4;
+    uint32_t skip_below, int find_first, uint32_t kChunk, unsigned long long* __restrict__ cursor,
+    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total) {
   extern __shared__ uint64_t sm[];
   const unsigned tid = threadIdx.x, lane = tid & 31u;
   uint64_t* cand = sm;
@@ -659,7 +658,8 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
   const bool tiles = data->adj_words == 1;
   int rc = SIGMO_OK;
   if (tiles) {
-    const uint64_t chunk = std::min<uint64_t>(m->total, 8ull << 20);
+    const sigmo_tuning& tn = q->tune;
+    const uint64_t chunk = std::min<uint64_t>(m->total, static_cast<uint64_t>(tn.mask_chunk_slots) << 20);
     void* mbuf = nullptr;
     rc = dev_alloc(q, &mbuf, 8ull * kPhaseLevels * chunk + 16ull * chunk);
     const size_t smem = static_cast<size_t>(kPhaseLevels) * kPhaseThreads * (2 * 8 + 1);
@@ -681,20 +681,25 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
         rc = fail(SIGMO_ERR_CUDA, "event record failed");
       if (!rc) {
         SIGMO_CUDA_TRY(cudaMemsetAsync(ctr, 0, 8, q->stream));
-        const unsigned grid = 148u * 3u;
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device);
+        const unsigned grid = static_cast<unsigned>(sms) * tn.join_blocks_per_sm;
         if (exact)
           k_join_masks<true><<<grid, kPhaseThreads, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id,
-                                                                         data->adj, skip, find_first, ctr, m->counts, tot);
+                                                                         data->adj, skip, find_first, tn.join_chunk, ctr,
+                                                                         m->counts, tot);
         else
           k_join_masks<false><<<grid, kPhaseThreads, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id,
-                                                                          data->adj, skip, find_first, ctr, m->counts, tot);
+                                                                          data->adj, skip, find_first, tn.join_chunk, ctr,
+                                                                          m->counts, tot);
         rc = check_launch(q, "k_join_masks");
       }
     }
     dev_free(q, mbuf);
   }
   const cudaStream_t main_stream = q->stream;
-  if (!rc && tiles) {
+  const bool side = tiles && !q->tune.overflow_serial;
+  if (!rc && side) {
     // the overflow list is complete after the last Phase A: its pairs run on
     // the side stream, overlapping Phase B (the caller joins the side stream)
     if (cudaStreamWaitEvent(q->side, q->ev_fork, 0) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
@@ -703,7 +708,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
   if (!rc) {
     // the overflow list (two-phase route) or every slot (otherwise) through the generic kernel
     const unsigned block = 128;
-    const unsigned grid = 148u * 8u;
+    const unsigned grid = tiles ? q->tune.overflow_blocks : 148u * 8u;
     const uint32_t* list = tiles ? overflow : nullptr;
     const unsigned long long* list_len = tiles ? ctr + 2 : nullptr;
 #define SIGMO_JOIN_PLANES(AWV, EX)                                                                                      \
@@ -721,7 +726,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
     rc = check_launch(q, "k_join_fast<planes>");
   }
   q->stream = main_stream;
-  if (tiles && cudaEventRecord(q->ev_join, q->side) == cudaSuccess) cudaStreamWaitEvent(q->stream, q->ev_join, 0);
+  if (side && cudaEventRecord(q->ev_join, q->side) == cudaSuccess) cudaStreamWaitEvent(q->stream, q->ev_join, 0);
   dev_free(q, buf);
   return rc;
 }

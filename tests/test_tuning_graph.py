@@ -1,0 +1,67 @@
+"""CUDA-graph replay of the batched form and the join autotuner.
+
+Graph mode (SIGMO_MATCH_CUDA_GRAPH) must give the same totals and per-pair
+counts as the ordinary call on every replay, and recapture when the inputs
+change; every launch shape the autotuner tries must give the same result.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import sigmo_b200 as sb
+
+pytestmark = pytest.mark.gpu
+
+R = 4
+
+
+def _graphs(queue, nd, nq, seed):
+    d = sb.generate_molecules(nd, 10, 40, seed=seed)
+    q = sb.generate_queries(nq, 3, 20, seed=seed + 1, skew_lo=5, skew_hi=12)
+    return q, d, sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)
+
+
+def test_graph_mode_replays_match_the_ordinary_call():
+    queue = sb.Queue(0)
+    q, d, qg, dg = _graphs(queue, 3000, 60, 1701)
+    ref_m = sb.GMCR(queue)
+    ref = sb.match_batched(queue, qg, dg, R, False, None, ref_m)
+    ref_counts = ref_m.getPairCounts()
+    gm = sb.GMCR(queue)
+    for call in range(4):  # run + capture, then replays
+        res = sb.match_batched(queue, qg, dg, R, False, None, gm, graph=True)
+        assert res["total_matches"] == ref["total_matches"], f"call {call}"
+        assert res["admitted_pairs"] == ref["admitted_pairs"]
+        assert np.array_equal(gm.getPairCounts(), ref_counts), f"call {call}"
+    # find-first on the same handle: a different key, so a new capture
+    ff = sb.match_batched(queue, qg, dg, R, True, None, gm, graph=True)
+    ff2 = sb.match_batched(queue, qg, dg, R, True, None, gm, graph=True)
+    assert ff["total_matches"] == ff2["total_matches"] == int((ref_counts > 0).sum())
+    # other data graphs on the same GMCR object
+    q2, d2, qg2, dg2 = _graphs(queue, 1200, 30, 1711)
+    want = oracle.run_pipeline(q2, d2, R, oracle.REF_PTX, False)
+    for _ in range(2):
+        r2 = sb.match_batched(queue, qg2, dg2, R, False, None, gm, graph=True)
+        assert r2["total_matches"] == want["total"]
+        assert np.array_equal(gm.getPairCounts(), want["per_pair"])
+
+
+def test_autotune_keeps_results_and_sets_the_queue():
+    queue = sb.Queue(0)
+    q, d, qg, dg = _graphs(queue, 4000, 80, 1721)
+    base = sb.match_batched(queue, qg, dg, R, False, None, sb.GMCR(queue))
+    t = sb.autotune(queue, qg, dg, R, False, reps=1)
+    assert t["ms_join"] > 0 and t["ms_join_default"] > 0
+    assert t["ms_join"] <= t["ms_join_default"] * 1.05
+    got = queue.get_tuning()
+    for k in ("join_blocks_per_sm", "join_chunk", "overflow_blocks", "overflow_serial", "mask_chunk_slots"):
+        assert got[k] == t[k]
+    after = sb.match_batched(queue, qg, dg, R, False, None, sb.GMCR(queue))
+    assert after["total_matches"] == base["total_matches"]
+    # explicit shapes, including the serial overflow path and small mask chunks
+    queue.set_tuning(join_blocks_per_sm=1, join_chunk=16, overflow_blocks=148, overflow_serial=1, mask_chunk_slots=1)
+    gm = sb.GMCR(queue)
+    r = sb.match_batched(queue, qg, dg, R, False, None, gm)
+    assert r["total_matches"] == base["total_matches"]
+    with pytest.raises(sb.SigmoError):
+        queue.set_tuning(join_blocks_per_sm=9)
