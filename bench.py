@@ -74,6 +74,7 @@ def parse_args():
     ap.add_argument("--serve-inflight", type=int, default=2)
     ap.add_argument("--no-graph", action="store_true", help="time ordinary calls instead of CUDA-graph replays")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default join launch shape")
+    ap.add_argument("--serving-only", action="store_true", help="run only the serving measurement (prints its JSON)")
     return ap.parse_args()
 
 
@@ -328,6 +329,10 @@ def run_sigmo(args, rank, world, local):
     q, d = make_workload(wl, rank)
     R = wl["R"]
     pairs = q.num_graphs * d.num_graphs
+    if args.serving_only:
+        if rank == 0:
+            print(json.dumps({"serving": run_serving(args, d, wl, local)}))
+        return
 
     queue = sb.Queue(local, profile=args.profile)
     qg, dg = sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)

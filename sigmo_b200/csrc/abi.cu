@@ -7,6 +7,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <mutex>
+#include <utility>
+#include <vector>
 #include <new>
 
 #include "internal.hpp"
@@ -24,6 +27,22 @@ int normalize_tuning(sigmo_tuning* t) {
   if (t->overflow_blocks > 65535) return fail(SIGMO_ERR_INVALID, "overflow_blocks must be <= 65535");
   if (t->overflow_serial > 1) return fail(SIGMO_ERR_INVALID, "overflow_serial must be 0 or 1");
   if (t->mask_chunk_slots > 64) return fail(SIGMO_ERR_INVALID, "mask_chunk_slots must be 1..64");
+  return SIGMO_OK;
+}
+
+int allow_max_dynamic_smem(const void* kernel, int device) {
+  static std::mutex mu;
+  static std::vector<std::pair<const void*, int>> done;
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto& d : done)
+    if (d.first == kernel && d.second == device) return SIGMO_OK;
+  int optin = 0;
+  SIGMO_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  cudaFuncAttributes fa{};
+  SIGMO_CUDA_TRY(cudaFuncGetAttributes(&fa, kernel));
+  SIGMO_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      optin - static_cast<int>(fa.sharedSizeBytes)));
+  done.emplace_back(kernel, device);
   return SIGMO_OK;
 }
 

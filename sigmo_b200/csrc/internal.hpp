@@ -155,6 +155,12 @@ inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap = 0x7FFFFFF
 
 int check_launch(Queue* q, const char* what);
 
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in maximum
+// once per (kernel, device).  Kernels launched with different dynamic sizes
+// from several host threads (the serving workers) must not lower it for one
+// another, so the limit is only ever set to the maximum.
+int allow_max_dynamic_smem(const void* kernel, int device);
+
 // ---- kernel launchers (defined in the .cu files) --------------------------
 int launch_graph_derive(Graph* g);
 int launch_query_order(Graph* g);

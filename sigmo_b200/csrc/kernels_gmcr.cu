@@ -14,6 +14,7 @@
 
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <mutex>
 
 #include "internal.hpp"
@@ -170,12 +171,14 @@ int launch_gmcr_from_admit(Queue* q, const Graph* query, const Graph* data, cons
     dev_free(q, m->counts);
     m->indices = m->pair_graph = nullptr;
     m->counts = nullptr;
+    // grow by half again at least, so a sequence of growing batches
+    // reallocates O(log) times
+    const uint64_t n = std::max<uint64_t>(cap ? cap : 1, m->capacity + m->capacity / 2);
     m->capacity = 0;
-    const uint64_t n = cap ? cap : 1;
     rc = dev_alloc(q, reinterpret_cast<void**>(&m->indices), sizeof(uint32_t) * n);
     if (!rc) rc = dev_alloc(q, reinterpret_cast<void**>(&m->pair_graph), sizeof(uint32_t) * n);
     if (!rc) rc = dev_alloc(q, reinterpret_cast<void**>(&m->counts), sizeof(uint64_t) * n);
-    if (!rc) m->capacity = cap;
+    if (!rc) m->capacity = n;
   }
   if (!rc && G && QG) {
     k_gmcr_fill<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(admit, GW, QG, G, m->offsets, m->indices,

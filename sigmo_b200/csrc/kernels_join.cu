@@ -663,12 +663,9 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
     void* mbuf = nullptr;
     rc = dev_alloc(q, &mbuf, 8ull * kPhaseLevels * chunk + 16ull * chunk);
     const size_t smem = static_cast<size_t>(kPhaseLevels) * kPhaseThreads * (2 * 8 + 1);
-    cudaError_t e = cudaSuccess;
-    if (!rc) {
-      e = exact ? cudaFuncSetAttribute(k_join_masks<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem))
-                : cudaFuncSetAttribute(k_join_masks<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-      if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "k_join_masks shared-memory setup failed: %s", cudaGetErrorString(e));
-    }
+    if (!rc)
+      rc = exact ? allow_max_dynamic_smem(reinterpret_cast<const void*>(k_join_masks<true>), q->device)
+                 : allow_max_dynamic_smem(reinterpret_cast<const void*>(k_join_masks<false>), q->device);
     for (uint64_t slot0 = 0; slot0 < m->total && !rc; slot0 += chunk) {
       const uint64_t cnt = std::min<uint64_t>(chunk, m->total - slot0);
       auto* masks = static_cast<uint64_t*>(mbuf);

@@ -388,8 +388,8 @@ int admit_launch(Queue* q, const Graph* query, const Graph* data, const uint64_t
   const unsigned block = 32u * kAdmitWarps;
   int per_sm = 0, sms = 0;
   SIGMO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device));
-  cudaError_t e = cudaFuncSetAttribute(k_planes_admit<AW, GATHER>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_planes_admit<AW, GATHER>, block, smem);
+  SIGMO_TRY(allow_max_dynamic_smem(reinterpret_cast<const void*>(k_planes_admit<AW, GATHER>), q->device));
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_planes_admit<AW, GATHER>, block, smem);
   if (e != cudaSuccess) return fail(SIGMO_ERR_CUDA, "k_planes_admit shared-memory setup failed: %s", cudaGetErrorString(e));
   const uint64_t grid = std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms);
   k_planes_admit<AW, GATHER><<<grid, block, smem, q->stream>>>(
@@ -486,8 +486,9 @@ int build_resident_planes(Queue* q, Graph* data, const uint64_t* sig_all, uint32
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device);
     const unsigned block = 32u * kAdmitWarps;
 #define SIGMO_BUILD(AWV)                                                                                             \
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_build_planes<AWV>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                                 static_cast<int>(smem));                                            \
+  if (e == cudaSuccess &&                                                                                             \
+      allow_max_dynamic_smem(reinterpret_cast<const void*>(k_build_planes<AWV>), q->device) != SIGMO_OK)               \
+    e = cudaErrorInvalidValue;                                                                                         \
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_planes<AWV>, block, smem);  \
   if (e == cudaSuccess)                                                                                              \
     k_build_planes<AWV><<<std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms), block, smem,      \

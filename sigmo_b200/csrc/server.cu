@@ -523,6 +523,19 @@ int sigmo_server_create(int device, const sigmo_host_graphs* database, const sig
     if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) return cleanup(fail(SIGMO_ERR_CUDA, "cudaMemGetInfo failed"));
     s->so.memory_budget = freeb / 2;
   }
+  // Warm the device memory pool: one allocation of a quarter of the budget,
+  // freed at once.  The pool keeps the memory (its release threshold is
+  // unlimited), so the batches' stream-ordered allocations are carved from it
+  // instead of mapping new memory while requests wait.
+  {
+    void* warm = nullptr;
+    const uint64_t want = std::min<uint64_t>(s->so.memory_budget / 4, 32ull << 30);
+    if (want && dev_alloc(s->q0, &warm, want) == SIGMO_OK) {
+      dev_free(s->q0, warm);
+      cudaStreamSynchronize(s->q0->stream);
+    }
+    cudaGetLastError();
+  }
   s->workers.resize(o.max_inflight);
   for (auto& w : s->workers) {
     rc = sigmo_queue_create(device, &s->opts, &w.q);
