@@ -657,11 +657,9 @@ int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t da
   if (!q || !query || !data || !c || !m || !num_matches) return fail(SIGMO_ERR_INVALID, "null argument");
   if (m->num_data_graphs != data->num_graphs || !m->offsets) return fail(SIGMO_ERR_INVALID, "GMCR was not generated for this data graph");
   SIGMO_TRY(set_device(q));
-  void* scratch = nullptr;
   SIGMO_TRY(stage_begin(q));
   uint64_t* d_total = nullptr;
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
-  (void)scratch;
   SIGMO_CUDA_TRY(cudaMemsetAsync(d_total, 0, 8, q->stream));
   int rc = launch_join_literal(q, query, data, c, m, find_first, 0, data->num_graphs, d_total, 0, 0xFFFFFFFFu);
   if (!rc) rc = stage_end(q);
