@@ -81,6 +81,11 @@ SIGMO_API int sigmo_host_graphs_slice(const sigmo_host_graphs* in, uint32_t firs
  * buf == NULL; *len receives the byte count). */
 SIGMO_API int sigmo_format_graphs(const sigmo_host_graphs* in, char* buf, size_t* len);
 SIGMO_API void sigmo_host_graphs_free(sigmo_host_graphs* g);
+/* Binary batches (no reference counterpart; the reference reads text only):
+ * the five arrays as they are, behind a header, so a database loads without
+ * parsing.  Loading checks sizes and offsets (SIGMO_ERR_FORMAT otherwise). */
+SIGMO_API int sigmo_graphs_save(const sigmo_host_graphs* in, const char* path);
+SIGMO_API int sigmo_graphs_load(const char* path, sigmo_host_graphs* out);
 
 /* ---- seeded synthetic inputs (stand-ins for the missing ZINC / SMARTS sets) */
 /* kind: 0 = drug-like molecules (sizes uniform in [min_atoms, max_atoms]),
@@ -150,6 +155,18 @@ SIGMO_API int sigmo_graph_create_device(sigmo_queue_t q, uint32_t num_graphs, ui
                               const uint32_t* d_graph_offsets, const uint32_t* d_row_offsets,
                               const uint32_t* d_column_indices, const uint8_t* d_node_labels,
                               const uint8_t* d_edge_labels, sigmo_graph_t* out);
+/* createDeviceCSRGraph with the batching done on the device (the reference
+ * concatenates on the host, graph.hpp:254-314, "TODO offload on GPU"): the
+ * graphs' own CSR arrays back to back with local ids — node_counts[g],
+ * edge_counts[g] (directed entries), each graph's n_g + 1 row pointers from 0
+ * (sum n_g + num_graphs entries), local neighbour ids, node and edge labels
+ * (edge_labels may be NULL: all 0).  Host arrays, copied as they are; offsets
+ * are scanned and ids rebased on the device.  SIGMO_ERR_INVALID if a local id
+ * or row pointer is outside its graph. */
+SIGMO_API int sigmo_graph_create_from_local(sigmo_queue_t q, uint32_t num_graphs, const uint32_t* node_counts,
+                                            const uint32_t* edge_counts, const uint32_t* row_offsets_local,
+                                            const uint32_t* columns_local, const uint8_t* node_labels,
+                                            const uint8_t* edge_labels, sigmo_graph_t* out);
 /* destroyDeviceCSRGraph (graph.hpp:316-322). */
 SIGMO_API int sigmo_graph_destroy(sigmo_graph_t g);
 SIGMO_API int sigmo_graph_info(sigmo_graph_t g, uint32_t* num_graphs, uint64_t* total_nodes, uint64_t* total_edges,
@@ -248,6 +265,16 @@ SIGMO_API int sigmo_gmcr_generate_noalloc(sigmo_queue_t q, sigmo_graph_t query, 
  * of every GMCR slot (total_query_indices entries). */
 SIGMO_API int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c,
                           sigmo_gmcr_t m, uint64_t* num_matches, int find_first, uint64_t* per_pair);
+/* joinWildcardCandidates (isomorphism.hpp:435-560, with defineMatchingOrder
+ * :383-408 and isValidMapping :410-433): the reference's opt-in join that
+ * roots each pair's DFS at the query vertex with the most candidates, splits
+ * the root's candidates over the 32 lanes of a sub-group and also requires
+ * equal bond (edge) labels on query edges.  The driver (sigmo.cpp) never calls
+ * it.  find_first ends each lane's DFS at its first match, so the count is
+ * then the number of root candidates that extend to a match.  per_pair: the
+ * count of every GMCR slot (nullable). */
+SIGMO_API int sigmo_join_wildcard_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c,
+                                             sigmo_gmcr_t m, uint64_t* num_matches, int find_first, uint64_t* per_pair);
 
 /* ---- batched form: whole pipeline in one call ----------------------------
  * Signatures for iterations 1..R in one BFS, per-data-graph candidate planes

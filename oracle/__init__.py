@@ -63,6 +63,8 @@ def lib():
         L.orc_join.restype = u64
         L.orc_join_closed_form.argtypes = [P, P, vp, vp, vp, i32, vp]
         L.orc_join_closed_form.restype = u64
+        L.orc_join_wildcard.argtypes = [P, vp, P, vp, vp, vp, vp, i32, i32, ctypes.c_uint32, vp]
+        L.orc_join_wildcard.restype = u64
         L.orc_sig_set.argtypes = [u64, u32, u32]
         L.orc_sig_set.restype = u64
         L.orc_sig_get.argtypes = [u64, u32]
@@ -258,6 +260,22 @@ def join_closed_form(qg, dg, bits, offsets, indices, find_first: bool = False):
                                        int(find_first), _ptr(per))
     return int(total), per[: len(indices)]
 
+
+
+def join_wildcard(qg, dg, bits, offsets, indices, profile: int = REF_PTX, find_first: bool = True, wg: int = 128):
+    """joinWildcardCandidates (isomorphism.hpp:435-560) on the final bitset and
+    GMCR: returns (total, per-slot counts)."""
+    q, d = as_batch(qg), as_batch(dg)
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+    idx = np.ascontiguousarray(indices, dtype=np.uint32)
+    per = np.zeros(max(int(offsets[-1]), 1), np.uint64)
+    qel = np.ascontiguousarray(q.edge_labels, dtype=np.uint8)
+    del_ = np.ascontiguousarray(d.edge_labels, dtype=np.uint8)
+    total = lib().orc_join_wildcard(ctypes.byref(_cg(q)), _ptr(qel), ctypes.byref(_cg(d)), _ptr(del_), _ptr(bits), _ptr(offsets),
+                                    _ptr(idx), profile, int(bool(find_first)), wg, _ptr(per))
+    if total == 2**64 - 1:
+        raise ValueError("outside the oracle's domain")
+    return int(total), per[: int(offsets[-1])]
 
 def run_pipeline(qg, dg, iterations: int, profile: int = REF_PTX, find_first: bool = False, wg: int = 128,
                  keep: bool = False, skip_join: bool = False):

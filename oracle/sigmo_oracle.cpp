@@ -546,6 +546,159 @@ uint64_t orc_join_closed_form(const orc_graph* q, const orc_graph* d, const uint
   return total;
 }
 
+// getEdgeLabel (graph.hpp:88-93): label of the CSR entry node -> nb, or 255
+// (label_t(-1)) when there is none.
+static inline uint8_t edge_label(const orc_graph* g, const uint8_t* el, uint32_t node, uint32_t nb) {
+  for (uint32_t i = g->row_offsets[node]; i < g->row_offsets[node + 1]; ++i)
+    if (g->column_indices[i] == nb) return el[i];
+  return 0xFFu;
+}
+
+// defineMatchingOrder + isValidMapping + joinWildcardCandidates
+// (isomorphism.hpp:383-560).  A work-group of `wg` items per data graph is cut
+// into sub-groups of 32; sub-group sg takes GMCR segment slots sg, sg + wg/32,
+// ...  For a slot, the matching order starts with the query vertex (among the
+// first 32) with the most range-masked candidates (the highest such id; the
+// reduce over the sub-group), then the others in identity order.  Lane l of
+// the sub-group runs one DFS per starting candidate l, l + 32, ... of that
+// root: frames {depth, next index} from depth 1, the uint8-indexed `visited`
+// bitset of the driver's join (cleared and re-seeded with the root whenever
+// the DFS returns to depth 1), and isValidMapping, which also requires equal
+// bond labels on query edges.  find_first ends a lane's DFS at its first
+// match, so the count is then the number of starting candidates that
+// extend.  mapping[] (indexed by query vertex) starts zeroed per work-item
+// and carries over between its DFS runs.  EXACT: injective with clean
+// backtracking.  per_pair[slot] = the slot's matches over all its lanes.
+// Returns the total, or UINT64_MAX outside the supported domain.
+uint64_t orc_join_wildcard(const orc_graph* q, const uint8_t* qel, const orc_graph* d, const uint8_t* del, const uint32_t* bits,
+                           const uint32_t* offsets, const uint32_t* indices, int prof, int find_first, uint32_t wg,
+                           uint64_t* per_pair) {
+  constexpr uint32_t kMaxDepth = 64, kSub = 32;
+  for (uint32_t qg = 0; qg < q->num_graphs; ++qg)
+    if (q->graph_offsets[qg + 1] - q->graph_offsets[qg] > kMaxDepth) return UINT64_MAX;
+  if (prof == ORC_EXACT)
+    for (uint32_t gi = 0; gi < d->num_graphs; ++gi)
+      if (d->graph_offsets[gi + 1] - d->graph_offsets[gi] > 64u * kExactWords) return UINT64_MAX;
+  if (wg == 0) wg = 128;
+  const uint32_t nsg = std::max<uint32_t>(1u, wg / kSub);
+  const uint64_t W = (d->total_nodes + 31) / 32;
+  Cand c{bits, W, prof};
+  if (per_pair) std::memset(per_pair, 0, sizeof(uint64_t) * offsets[d->num_graphs]);
+  uint64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total)
+  for (int64_t gi = 0; gi < static_cast<int64_t>(d->num_graphs); ++gi) {
+    const uint32_t s = d->graph_offsets[gi], e = d->graph_offsets[gi + 1];
+    const uint32_t seg0 = offsets[gi], seglen = offsets[gi + 1] - offsets[gi];
+    for (uint32_t sg = 0; sg < nsg; ++sg) {
+      for (uint32_t lane = 0; lane < kSub; ++lane) {
+        uint32_t mapping[kMaxDepth];
+        std::memset(mapping, 0, sizeof(mapping));
+        for (uint32_t it = sg; it < seglen; it += nsg) {
+          const uint32_t qg = indices[seg0 + it];
+          const uint32_t qoff = q->graph_offsets[qg];
+          const uint32_t n = q->graph_offsets[qg + 1] - qoff;
+          // defineMatchingOrder (isomorphism.hpp:383-408)
+          uint32_t max_c = 0;
+          int root = -1;
+          const uint32_t lanes = std::min<uint32_t>(n, kSub);
+          for (uint32_t i = 0; i < lanes; ++i) max_c = std::max(max_c, c.count(qoff + i, s, e));
+          for (uint32_t i = 0; i < lanes; ++i)
+            if (c.count(qoff + i, s, e) == max_c) root = static_cast<int>(i);
+          uint32_t order[kMaxDepth];
+          order[0] = static_cast<uint32_t>(root);
+          for (uint32_t i = 0, j = 1; i < n; ++i)
+            if (static_cast<int>(i) != root) order[j++] = i;
+          auto valid = [&](uint32_t cand, uint32_t depth) {
+            for (uint32_t i = 0; i < depth; ++i) {
+              const bool qa = is_neighbor(q, order[i] + qoff, order[depth] + qoff);
+              if (qa != is_neighbor(d, mapping[order[i]], cand)) return false;
+              if (qa && edge_label(d, del, mapping[order[i]], cand) != edge_label(q, qel, order[i] + qoff, order[depth] + qoff))
+                return false;
+            }
+            return true;
+          };
+          uint64_t found = 0;
+          for (uint32_t sc = lane; sc < max_c; sc += kSub) {
+            struct Frame { uint32_t depth, idx; } stack[kMaxDepth + 2];
+            uint32_t top = 0;
+            const uint32_t r = order[0];
+            mapping[r] = c.at(qoff + r, sc, s, e);
+            stack[top++] = {1, 0};
+            if (prof != ORC_EXACT) {
+              RefBitset visited;
+              visited.offset = s;
+              visited.prof = prof;
+              visited.set(mapping[r]);
+              while (top > 0) {
+                const Frame fr = stack[top - 1];
+                if (fr.depth == n) {
+                  ++found;
+                  --top;
+                  if (find_first) break;
+                  continue;
+                }
+                const uint32_t qn = order[fr.depth];
+                if (fr.idx >= c.count(qn + qoff, s, e)) {
+                  --top;
+                  visited.unset(mapping[qn]);
+                  if (top == 1) {
+                    visited.data = 0;
+                    visited.set(mapping[r]);
+                  }
+                  continue;
+                }
+                const uint32_t cand = c.at(qn + qoff, fr.idx, s, e);
+                stack[top - 1].idx++;
+                if (visited.get(cand)) continue;
+                if (valid(cand, fr.depth)) {
+                  mapping[qn] = cand;
+                  visited.set(cand);
+                  stack[top++] = {fr.depth + 1, 0};
+                }
+              }
+            } else {
+              WideSet used;
+              uint32_t placed[kMaxDepth + 1];
+              for (uint32_t k = 0; k <= kMaxDepth; ++k) placed[k] = 0xFFFFFFFFu;
+              used.set(mapping[r] - s);
+              while (top > 0) {
+                const Frame fr = stack[top - 1];
+                if (fr.depth == n) {
+                  ++found;
+                  --top;
+                  if (find_first) break;
+                  continue;
+                }
+                if (placed[fr.depth] != 0xFFFFFFFFu) {  // resuming: undo this depth's last placement
+                  used.unset(placed[fr.depth] - s);
+                  placed[fr.depth] = 0xFFFFFFFFu;
+                }
+                const uint32_t qn = order[fr.depth];
+                if (fr.idx >= c.count(qn + qoff, s, e)) {
+                  --top;
+                  continue;
+                }
+                const uint32_t cand = c.at(qn + qoff, fr.idx, s, e);
+                stack[top - 1].idx++;
+                if (used.get(cand - s)) continue;
+                if (valid(cand, fr.depth)) {
+                  mapping[qn] = cand;
+                  placed[fr.depth] = cand;
+                  used.set(cand - s);
+                  stack[top++] = {fr.depth + 1, 0};
+                }
+              }
+            }
+          }
+          if (per_pair) per_pair[seg0 + it] += found;
+          total += found;
+        }
+      }
+    }
+  }
+  return total;
+}
+
 // SignatureDevice methods, exported for the reference's signature KAT
 // (library/test/candidates.cpp:13-32).
 uint64_t orc_sig_set(uint64_t s, uint32_t label, uint32_t count) { return sig_set(s, label, count); }

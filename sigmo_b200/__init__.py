@@ -121,6 +121,32 @@ class HostGraphs:
         check(lib().sigmo_format_graphs(ctypes.byref(self._raw), buf, ctypes.byref(n)))
         return buf.raw[: n.value].decode()
 
+    def save(self, path) -> None:
+        """Binary batch file (sigmo_graphs_save)."""
+        check(lib().sigmo_graphs_save(ctypes.byref(self._raw), str(path).encode()))
+
+    @staticmethod
+    def load(path) -> "HostGraphs":
+        out = _L.HostGraphsC()
+        check(lib().sigmo_graphs_load(str(path).encode(), ctypes.byref(out)))
+        return HostGraphs(out)
+
+    def local_arrays(self):
+        """The batch as per-graph CSRs back to back with local ids (the input
+        of createDeviceCSRGraphFromLocal): node counts, directed-edge counts,
+        each graph's n+1 row pointers from 0, local neighbour ids."""
+        goff = self.graph_offsets.astype(np.int64)
+        roff = self.row_offsets.astype(np.int64)
+        n = np.diff(goff)
+        e = roff[goff[1:]] - roff[goff[:-1]]
+        # row pointers: graph g contributes roff[goff[g] .. goff[g+1]] - roff[goff[g]]
+        idx = np.concatenate([np.arange(a, b + 1) for a, b in zip(goff[:-1], goff[1:])]) if len(n) else np.zeros(0, np.int64)
+        base = np.repeat(roff[goff[:-1]], n + 1)
+        rows = (roff[idx] - base).astype(np.uint32)
+        gof_edge = np.repeat(goff[:-1], e)
+        cols = (self.column_indices.astype(np.int64) - gof_edge).astype(np.uint32)
+        return n.astype(np.uint32), e.astype(np.uint32), rows, cols
+
     @staticmethod
     def from_text(text: str) -> "HostGraphs":
         data = text.encode()
@@ -266,6 +292,18 @@ class DeviceBatchedCSRGraph:
 def createDeviceCSRGraph(queue: Queue, graphs: HostGraphs) -> DeviceBatchedCSRGraph:
     h = ctypes.c_void_p()
     check(lib().sigmo_graph_create(queue._h, ctypes.byref(graphs._raw), ctypes.byref(h)))
+    return DeviceBatchedCSRGraph(queue, h)
+
+
+def createDeviceCSRGraphFromLocal(queue: Queue, graphs: HostGraphs) -> DeviceBatchedCSRGraph:
+    """createDeviceCSRGraph with the concatenation on the device
+    (sigmo_graph_create_from_local), from the batch's per-graph local arrays."""
+    n, e, rows, cols = graphs.local_arrays()
+    nl = np.ascontiguousarray(graphs.node_labels)
+    el = np.ascontiguousarray(graphs.edge_labels)
+    h = ctypes.c_void_p()
+    check(lib().sigmo_graph_create_from_local(queue._h, graphs.num_graphs, n.ctypes.data, e.ctypes.data, rows.ctypes.data,
+                                              cols.ctypes.data, nl.ctypes.data, el.ctypes.data, ctypes.byref(h)))
     return DeviceBatchedCSRGraph(queue, h)
 
 
@@ -473,6 +511,23 @@ def joinCandidates(queue: Queue, query_graphs, data_graphs, candidates: Candidat
     return ev
 
 
+def joinWildcardCandidates(queue: Queue, query_graphs, data_graphs, candidates: Candidates, gmcr: GMCR, num_matches,
+                           find_first: bool = True, per_pair: bool = False):
+    """isomorphism::join::joinWildcardCandidates (isomorphism.hpp:435-560):
+    max-candidate root, the root's candidates split over a sub-group's lanes,
+    bond labels checked.  Same arguments and result as joinCandidates."""
+    acc = ctypes.c_uint64(int(num_matches[0]))
+    pp = np.zeros(max(gmcr.total_query_indices, 1), np.uint64) if per_pair else None
+    check(lib().sigmo_join_wildcard_candidates(queue._h, query_graphs._h, data_graphs._h, candidates._h, gmcr._h,
+                                               ctypes.byref(acc), int(bool(find_first)),
+                                               pp.ctypes.data_as(ctypes.c_void_p) if pp is not None else None))
+    num_matches[0] = acc.value
+    ev = BatchedEvent(queue)
+    if per_pair:
+        return ev, pp[: gmcr.total_query_indices]
+    return ev
+
+
 MATCH_MATERIALIZE_BITSET = 1
 
 
@@ -590,5 +645,5 @@ signature = SimpleNamespace(Signature=Signature)
 isomorphism = SimpleNamespace(
     filter=SimpleNamespace(filterCandidates=filterCandidates, refineCandidates=refineCandidates),
     mapping=SimpleNamespace(GMCR=GMCR),
-    join=SimpleNamespace(joinCandidates=joinCandidates),
+    join=SimpleNamespace(joinCandidates=joinCandidates, joinWildcardCandidates=joinWildcardCandidates),
 )

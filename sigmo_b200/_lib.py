@@ -115,6 +115,9 @@ SIGNATURES = {
     "sigmo_host_graphs_slice": (_i, [_P(HostGraphsC), _u32, _u32, _P(HostGraphsC)]),
     "sigmo_format_graphs": (_i, [_P(HostGraphsC), _vp, _P(_sz)]),
     "sigmo_host_graphs_free": (None, [_P(HostGraphsC)]),
+    "sigmo_graphs_save": (_i, [_P(HostGraphsC), ctypes.c_char_p]),
+    "sigmo_graphs_load": (_i, [ctypes.c_char_p, _P(HostGraphsC)]),
+    "sigmo_graph_create_from_local": (_i, [_vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _P(_vp)]),
     "sigmo_generate_molecules": (_i, [_i, _u32, _u32, _u32, _d, _u64, _P(HostGraphsC)]),
     "sigmo_generate_queries": (_i, [_i, _u32, _u32, _u32, _u32, _u32, _u64, _P(HostGraphsC)]),
     "sigmo_default_options": (None, [_P(OptionsC)]),
@@ -152,6 +155,7 @@ SIGNATURES = {
     "sigmo_gmcr_download": (_i, [_vp, _vp, _u64, _vp, _u64]),
     "sigmo_gmcr_generate_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _u64, _P(_u64)]),
     "sigmo_join_candidates": (_i, [_vp, _vp, _vp, _vp, _vp, _P(_u64), _i, _vp]),
+    "sigmo_join_wildcard_candidates": (_i, [_vp, _vp, _vp, _vp, _vp, _P(_u64), _i, _vp]),
     "sigmo_match_batched": (_i, [_vp, _vp, _vp, _u32, _i, _u32, _vp, _vp, _P(MatchResultC)]),
     "sigmo_queue_set_tuning": (_i, [_vp, _P(TuningC)]),
     "sigmo_queue_get_tuning": (_i, [_vp, _P(TuningC)]),

@@ -98,6 +98,8 @@ int set_device(Queue* q) {
   return SIGMO_OK;
 }
 
+}  // namespace
+
 int finish_graph(Graph* g) {
   static std::atomic<uint64_t> next_stamp{1};
   g->stamp = next_stamp++;
@@ -112,7 +114,6 @@ int finish_graph(Graph* g) {
   return launch_graph_derive(g);
 }
 
-}  // namespace
 }  // namespace sigmo_b200
 
 using namespace sigmo_b200;
@@ -662,6 +663,33 @@ int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t da
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
   SIGMO_CUDA_TRY(cudaMemsetAsync(d_total, 0, 8, q->stream));
   int rc = launch_join_literal(q, query, data, c, m, find_first, 0, data->num_graphs, d_total, 0, 0xFFFFFFFFu);
+  if (!rc) rc = stage_end(q);
+  if (!rc) {
+    cudaError_t e = cudaMemcpyAsync(q->pinned, d_total, 8, cudaMemcpyDeviceToHost, q->stream);
+    if (e == cudaSuccess && per_pair && m->total) e = cudaMemcpyAsync(per_pair, m->counts, 8 * m->total, cudaMemcpyDeviceToHost, q->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(q->stream);
+    if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "join read-back failed: %s", cudaGetErrorString(e));
+    else {
+      *num_matches += *static_cast<uint64_t*>(q->pinned);
+      m->counts_valid = true;
+    }
+  }
+  dev_free(q, d_total);
+  return rc;
+}
+
+// joinWildcardCandidates (isomorphism.hpp:435-560): bond-label-aware join,
+// off the driver path (sigmo.cpp never calls it).
+int sigmo_join_wildcard_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c, sigmo_gmcr_t m,
+                          uint64_t* num_matches, int find_first, uint64_t* per_pair) {
+  if (!q || !query || !data || !c || !m || !num_matches) return fail(SIGMO_ERR_INVALID, "null argument");
+  if (m->num_data_graphs != data->num_graphs || !m->offsets) return fail(SIGMO_ERR_INVALID, "GMCR was not generated for this data graph");
+  SIGMO_TRY(set_device(q));
+  SIGMO_TRY(stage_begin(q));
+  uint64_t* d_total = nullptr;
+  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
+  SIGMO_CUDA_TRY(cudaMemsetAsync(d_total, 0, 8, q->stream));
+  int rc = launch_join_wildcard(q, query, data, c, m, find_first, d_total);
   if (!rc) rc = stage_end(q);
   if (!rc) {
     cudaError_t e = cudaMemcpyAsync(q->pinned, d_total, 8, cudaMemcpyDeviceToHost, q->stream);

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cerrno>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -313,6 +314,78 @@ int sigmo_format_graphs(const sigmo_host_graphs* in, char* buf, size_t* len) {
     std::memcpy(buf, s.data(), s.size());
   }
   *len = s.size();
+  return SIGMO_OK;
+}
+
+// ---- binary batches ---------------------------------------------------------
+// Layout (little-endian): "SIGMOCSR", u32 version (1), u32 num_graphs,
+// u64 total_nodes, u64 total_edges, then graph_offsets[G+1], row_offsets[N+1],
+// column_indices[E] (u32), node_labels[N], edge_labels[E] (u8).  Loading
+// checks every size and offset, so a damaged file is an error, not a batch.
+int sigmo_graphs_save(const sigmo_host_graphs* in, const char* path) {
+  if (!in || !path) return fail(SIGMO_ERR_INVALID, "sigmo_graphs_save: null argument");
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(SIGMO_ERR_INVALID, "cannot open %s for writing", path);
+  const char magic[8] = {'S', 'I', 'G', 'M', 'O', 'C', 'S', 'R'};
+  const uint32_t head[2] = {1u, in->num_graphs};
+  const uint64_t sizes[2] = {in->total_nodes, in->total_edges};
+  bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(head, 4, 2, f) == 2 && std::fwrite(sizes, 8, 2, f) == 2;
+  auto put = [&](const void* p, size_t elem, uint64_t n) {
+    if (ok && n) ok = std::fwrite(p, elem, n, f) == n;
+  };
+  put(in->graph_offsets, 4, in->num_graphs + 1ull);
+  put(in->row_offsets, 4, in->total_nodes + 1);
+  put(in->column_indices, 4, in->total_edges);
+  put(in->node_labels, 1, in->total_nodes);
+  put(in->edge_labels, 1, in->total_edges);
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? SIGMO_OK : fail(SIGMO_ERR_INVALID, "writing %s failed", path);
+}
+
+int sigmo_graphs_load(const char* path, sigmo_host_graphs* out) {
+  if (!path || !out) return fail(SIGMO_ERR_INVALID, "sigmo_graphs_load: null argument");
+  std::memset(out, 0, sizeof(*out));
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(SIGMO_ERR_INVALID, "cannot open %s", path);
+  char magic[8];
+  uint32_t head[2];
+  uint64_t sizes[2];
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "SIGMOCSR", 8) == 0 && std::fread(head, 4, 2, f) == 2 &&
+            head[0] == 1u && std::fread(sizes, 8, 2, f) == 2 && sizes[0] < (1ull << 32) && sizes[1] < (1ull << 32);
+  if (!ok) {
+    std::fclose(f);
+    return fail(SIGMO_ERR_FORMAT, "%s is not a sigmo_b200 binary batch (version 1)", path);
+  }
+  if (!alloc_host_graphs(out, head[1], sizes[0], sizes[1])) {
+    std::fclose(f);
+    return fail(SIGMO_ERR_OOM, "host allocation of a %llu-vertex batch failed", (unsigned long long)sizes[0]);
+  }
+  auto get = [&](void* p, size_t elem, uint64_t n) {
+    if (ok && n) ok = std::fread(p, elem, n, f) == n;
+  };
+  get(out->graph_offsets, 4, out->num_graphs + 1ull);
+  get(out->row_offsets, 4, out->total_nodes + 1);
+  get(out->column_indices, 4, out->total_edges);
+  get(out->node_labels, 1, out->total_nodes);
+  get(out->edge_labels, 1, out->total_edges);
+  std::fclose(f);
+  // structural checks: offsets start at 0, never decrease and end at the
+  // totals; neighbours stay inside their graph
+  if (ok) ok = out->graph_offsets[0] == 0 && out->graph_offsets[out->num_graphs] == out->total_nodes && out->row_offsets[0] == 0 &&
+               out->row_offsets[out->total_nodes] == out->total_edges;
+  for (uint32_t g = 0; ok && g < out->num_graphs; ++g) {
+    const uint32_t v0 = out->graph_offsets[g], v1 = out->graph_offsets[g + 1];
+    if (v1 < v0) ok = false;
+    for (uint32_t v = v0; ok && v < v1; ++v) {
+      if (out->row_offsets[v + 1] < out->row_offsets[v]) ok = false;
+      for (uint32_t i = out->row_offsets[v]; ok && i < out->row_offsets[v + 1]; ++i)
+        if (out->column_indices[i] < v0 || out->column_indices[i] >= v1) ok = false;
+    }
+  }
+  if (!ok) {
+    sigmo_host_graphs_free(out);
+    return fail(SIGMO_ERR_FORMAT, "%s is truncated or inconsistent", path);
+  }
   return SIGMO_OK;
 }
 

@@ -163,6 +163,9 @@ int allow_max_dynamic_smem(const void* kernel, int device);
 
 // ---- kernel launchers (defined in the .cu files) --------------------------
 int launch_graph_derive(Graph* g);
+// Sizes, low-offset count and the derived arrays of a new device graph whose
+// host_graph_offsets and device arrays are set.
+int finish_graph(Graph* g);
 int launch_query_order(Graph* g);
 int launch_sig_generate(Queue* q, const Graph* g, uint64_t* sig);
 int launch_sig_refine(Queue* q, const Graph* g, uint32_t view, uint64_t* sig, uint64_t* reach, uint32_t reach_words);
@@ -179,6 +182,8 @@ int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const C
                         uint32_t graph_begin, uint32_t graph_end, uint64_t* d_total, uint32_t q_begin, uint32_t q_end);
 int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
                      uint64_t* d_total);
+int launch_join_wildcard(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
+                         uint64_t* d_total);
 // planes: [graph / 32][planes_rows][AW][32]; prog: the class programs as
 // row indices into it (pp.prog for the per-batch planes).
 int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, const PlaneProgram& pp, const uint64_t* planes,

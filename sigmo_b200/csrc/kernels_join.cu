@@ -277,6 +277,158 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
   }
 }
 
+// getEdgeLabel (graph.hpp:88-93): label of the CSR entry a -> b, or 255.
+__device__ __forceinline__ uint8_t csr_edge_label(uint32_t a, uint32_t b, const uint32_t* __restrict__ roff,
+                                                  const uint32_t* __restrict__ col, const uint8_t* __restrict__ el) {
+  for (uint32_t i = roff[a]; i < roff[a + 1]; ++i)
+    if (col[i] == b) return el[i];
+  return 0xFFu;
+}
+
+// joinWildcardCandidates (isomorphism.hpp:435-560) with defineMatchingOrder
+// (:383-408) and the bond-label isValidMapping (:410-433).  A block is the
+// reference's work-group of join_work_group_size items, one data graph at a
+// time; warp w is sub-group w and takes GMCR segment slots w, w + warps, ...
+// For a slot the warp picks the root (the query vertex among the first 32
+// with the most candidates, highest id on ties: two warp max-reductions), and
+// lane l runs one DFS per starting candidate l, l + 32, ... of the root, with
+// the driver join's `visited` bitset (cleared and re-seeded with the root when
+// the DFS is back at depth 1) or, for EXACT, an injective set with clean
+// backtracking.  find_first ends a lane's DFS at its first match.  mapping[]
+// (per query vertex) starts zeroed per lane and carries over between its DFS
+// runs, as the reference's private array does.
+template <bool EXACT>
+__global__ void k_join_wildcard(const uint32_t* __restrict__ bits, uint64_t Wp, int prof, const uint32_t* __restrict__ qgoff,
+                                const uint64_t* __restrict__ qadj, const uint32_t* __restrict__ qroff,
+                                const uint32_t* __restrict__ qcol, const uint8_t* __restrict__ qel,
+                                const uint32_t* __restrict__ dgoff, const uint64_t* __restrict__ dadj, uint32_t dAW,
+                                const uint32_t* __restrict__ droff, const uint32_t* __restrict__ dcol,
+                                const uint8_t* __restrict__ del, const uint32_t* __restrict__ offsets,
+                                const uint32_t* __restrict__ indices, uint32_t G, int find_first,
+                                uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total) {
+  const unsigned lane = threadIdx.x & 31u, sg = threadIdx.x >> 5, nsg = blockDim.x >> 5;
+  uint64_t my_total = 0;
+  PairCands pc;
+  uint32_t mapping[kMaxQueryNodes];
+#pragma unroll 1
+  for (uint32_t k = 0; k < kMaxQueryNodes; ++k) mapping[k] = 0;
+  uint8_t order[kMaxQueryNodes];
+  for (uint32_t g = blockIdx.x; g < G; g += gridDim.x) {
+    const uint32_t s = dgoff[g], e = dgoff[g + 1], ng = e - s;
+    const bool small = ng <= 64u;
+    const uint32_t seg0 = offsets[g], seglen = offsets[g + 1] - seg0;
+    for (uint32_t it = sg; it < seglen; it += nsg) {
+      const uint32_t qg = indices[seg0 + it];
+      const uint32_t qoff = qgoff[qg], n = qgoff[qg + 1] - qoff;
+      if (small) pc.load(bits, Wp, qoff, n, s, e, prof);
+      auto count_of = [&](uint32_t qn) -> uint32_t {
+        return small ? pc.cnt[qn] : cand_count(bits + static_cast<uint64_t>(qoff + qn) * Wp, s, e, prof);
+      };
+      auto cand_of = [&](uint32_t qn, uint32_t idx) -> uint32_t {
+        return small ? pc.at(qn, idx) : cand_at(bits + static_cast<uint64_t>(qoff + qn) * Wp, idx, s, e, prof);
+      };
+      // defineMatchingOrder: lane i holds query vertex i (< 32)
+      const uint32_t mine = lane < n ? count_of(lane) : 0u;
+      const uint32_t max_c = __reduce_max_sync(0xFFFFFFFFu, mine);
+      const int root = __reduce_max_sync(0xFFFFFFFFu, (lane < n && mine == max_c) ? static_cast<int>(lane) : -1);
+      order[0] = static_cast<uint8_t>(root);
+#pragma unroll 1
+      for (uint32_t i = 0, j = 1; i < n; ++i)
+        if (static_cast<int>(i) != root) order[j++] = static_cast<uint8_t>(i);
+      auto valid = [&](uint32_t cand, uint32_t depth) -> bool {
+        const uint32_t qd = order[depth];
+        for (uint32_t i = 0; i < depth; ++i) {
+          const uint32_t qi = order[i];
+          const bool qa = (qadj[qoff + qi] >> qd) & 1ull;
+          if (qa != data_neighbor(mapping[qi], cand, s, ng, dadj, dAW, droff, dcol)) return false;
+          if (qa && csr_edge_label(mapping[qi], cand, droff, dcol, del) != csr_edge_label(qoff + qi, qoff + qd, qroff, qcol, qel))
+            return false;
+        }
+        return true;
+      };
+      uint64_t found = 0;
+      for (uint32_t sc = lane; sc < max_c; sc += 32u) {
+        Frame stack[kMaxQueryNodes + 2];
+        uint32_t top = 0;
+        const uint32_t r = order[0];
+        mapping[r] = cand_of(r, sc);
+        stack[top++] = {1u, 0u};
+        if (!EXACT) {
+          uint64_t visited = refbit(mapping[r], s);  // Bitset<uint64_t>{offset = s}
+          while (top > 0) {
+            const Frame fr = stack[top - 1];
+            if (fr.depth == n) {
+              ++found;
+              --top;
+              if (find_first) break;
+              continue;
+            }
+            const uint32_t qn = order[fr.depth];
+            if (fr.idx >= count_of(qn)) {
+              --top;
+              visited &= ~refbit(mapping[qn], s);
+              if (top == 1) visited = refbit(mapping[r], s);
+              continue;
+            }
+            const uint32_t cand = cand_of(qn, fr.idx);
+            stack[top - 1].idx++;
+            if (visited & refbit(cand, s)) continue;
+            if (valid(cand, fr.depth)) {
+              mapping[qn] = cand;
+              visited |= refbit(cand, s);
+              stack[top++] = {fr.depth + 1, 0u};
+            }
+          }
+        } else {
+          uint64_t used[kMaxAdjWords] = {0, 0, 0, 0};
+          uint32_t placed[kMaxQueryNodes + 1];
+#pragma unroll 1
+          for (uint32_t k = 0; k <= n; ++k) placed[k] = 0xFFFFFFFFu;
+          {
+            const uint32_t t = mapping[r] - s;
+            used[t >> 6] |= 1ull << (t & 63u);
+          }
+          while (top > 0) {
+            const Frame fr = stack[top - 1];
+            if (fr.depth == n) {
+              ++found;
+              --top;
+              if (find_first) break;
+              continue;
+            }
+            if (placed[fr.depth] != 0xFFFFFFFFu) {
+              const uint32_t t = placed[fr.depth] - s;
+              used[t >> 6] &= ~(1ull << (t & 63u));
+              placed[fr.depth] = 0xFFFFFFFFu;
+            }
+            const uint32_t qn = order[fr.depth];
+            if (fr.idx >= count_of(qn)) {
+              --top;
+              continue;
+            }
+            const uint32_t cand = cand_of(qn, fr.idx);
+            stack[top - 1].idx++;
+            const uint32_t t = cand - s;
+            if ((used[t >> 6] >> (t & 63u)) & 1ull) continue;
+            if (valid(cand, fr.depth)) {
+              mapping[qn] = cand;
+              placed[fr.depth] = cand;
+              used[t >> 6] |= 1ull << (t & 63u);
+              stack[top++] = {fr.depth + 1, 0u};
+            }
+          }
+        }
+      }
+      my_total += found;
+      uint64_t slot_total = found;
+      for (int o = 16; o; o >>= 1) slot_total += __shfl_xor_sync(0xFFFFFFFFu, slot_total, o);
+      if (lane == 0 && counts) counts[seg0 + it] = slot_total;
+    }
+  }
+  for (int o = 16; o; o >>= 1) my_total += __shfl_xor_sync(0xFFFFFFFFu, my_total, o);
+  if (lane == 0 && my_total) atomicAdd(d_total, static_cast<unsigned long long>(my_total));
+}
+
 // Graph-local candidate set of one bitset row for data graph [s, e): bit t =
 // global candidate s + t, after the profile's range masks.
 template <int AW>
@@ -606,6 +758,34 @@ int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const C
                                                        data->column_indices, m->offsets, m->indices, graph_begin, graph_end,
                                                        q_begin, q_end, find_first, m->counts, tot);
   return check_launch(q, "k_join_literal");
+}
+
+int launch_join_wildcard(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
+                         uint64_t* d_total) {
+  if (query->max_nodes > kMaxQueryNodes)
+    return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
+  const bool exact = q->opts.profile == kProfileExact;
+  if (exact && data->max_nodes > 64u * kMaxAdjWords)
+    return fail(SIGMO_ERR_DOMAIN, "exact profile supports data graphs of at most %u vertices", 64u * kMaxAdjWords);
+  const uint32_t wg = q->opts.join_work_group_size ? q->opts.join_work_group_size : 128u;
+  if (wg > 1024u || (wg & 31u)) return fail(SIGMO_ERR_INVALID, "join work-group size %u must be a multiple of 32 <= 1024", wg);
+  const uint32_t G = data->num_graphs;
+  if (!G) return SIGMO_OK;
+  const unsigned grid = std::min<uint32_t>(G, 148u * 64u);
+  auto* tot = reinterpret_cast<unsigned long long*>(d_total);
+  if (exact)
+    k_join_wildcard<true><<<grid, wg, 0, q->stream>>>(c->bits, c->Wp, q->opts.profile, query->graph_offsets, query->adj,
+                                                      query->row_offsets, query->column_indices, query->edge_labels,
+                                                      data->graph_offsets, data->adj, data->adj_words, data->row_offsets,
+                                                      data->column_indices, data->edge_labels, m->offsets, m->indices, G,
+                                                      find_first, m->counts, tot);
+  else
+    k_join_wildcard<false><<<grid, wg, 0, q->stream>>>(c->bits, c->Wp, q->opts.profile, query->graph_offsets, query->adj,
+                                                       query->row_offsets, query->column_indices, query->edge_labels,
+                                                       data->graph_offsets, data->adj, data->adj_words, data->row_offsets,
+                                                       data->column_indices, data->edge_labels, m->offsets, m->indices, G,
+                                                       find_first, m->counts, tot);
+  return check_launch(q, "k_join_wildcard");
 }
 
 int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,

@@ -158,3 +158,39 @@ def test_queue_without_gpu_is_an_error_not_a_fallback():
     with pytest.raises(sb.SigmoError) as ei:
         sb.Queue(0)
     assert ei.value.code == 6
+
+
+def test_binary_batch_roundtrip_and_damage(tmp_path):
+    g = sb.generate_molecules(300, 5, 40, seed=4401, kind=1, median=18.0)
+    path = tmp_path / "batch.bin"
+    g.save(path)
+    h = sb.HostGraphs.load(path)
+    for f in ("graph_offsets", "row_offsets", "column_indices", "node_labels", "edge_labels"):
+        assert np.array_equal(getattr(g, f), getattr(h, f)), f
+    raw = path.read_bytes()
+    (tmp_path / "short.bin").write_bytes(raw[: len(raw) // 2])
+    with pytest.raises(sb.SigmoError) as ei:
+        sb.HostGraphs.load(tmp_path / "short.bin")
+    assert ei.value.code == 5
+    bad = bytearray(raw)
+    bad[-(g.total_edges * 5 + g.total_nodes) - 4:-(g.total_edges * 5 + g.total_nodes)] = (10**9).to_bytes(4, "little")
+    (tmp_path / "bad.bin").write_bytes(bytes(bad))
+    with pytest.raises(sb.SigmoError):
+        sb.HostGraphs.load(tmp_path / "bad.bin")
+    with pytest.raises(sb.SigmoError):
+        sb.HostGraphs.load(tmp_path / "missing.bin")
+
+
+def test_local_arrays_rebuild_the_batch():
+    g = sb.generate_molecules(200, 3, 30, seed=4402)
+    n, e, rows, cols = g.local_arrays()
+    goff = np.concatenate([[0], np.cumsum(n.astype(np.int64))])
+    ebase = np.concatenate([[0], np.cumsum(e.astype(np.int64))])
+    # global row pointers and neighbour ids from the local arrays
+    rr = []
+    for k in range(len(n)):
+        start = goff[k] + k
+        rr.append(rows[start:start + n[k]].astype(np.int64) + ebase[k])
+    rr.append([ebase[-1]])
+    assert np.array_equal(np.concatenate(rr), g.row_offsets.astype(np.int64))
+    assert np.array_equal(cols.astype(np.int64) + np.repeat(goff[:-1], e), g.column_indices.astype(np.int64))

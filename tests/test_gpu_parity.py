@@ -243,3 +243,64 @@ def test_mid_size_slice_against_oracle():
         ref = _oracle(qh, dh, 6, oracle.REF_PTX, ff)
         _check(run_both_batched(qh, dh, 6, oracle.REF_PTX, ff), ref, f"batched ff={ff}")
         _check(run_plain(qh, dh, 6, oracle.REF_PTX, ff), ref, f"plain ff={ff}")
+
+
+@pytest.mark.gpu
+def test_device_batch_assembly_matches_host_batching():
+    d = sb.generate_molecules(3000, 5, 60, seed=4501, kind=1, median=20.0)
+    q = sb.generate_queries(40, 3, 12, seed=4502)
+    queue = sb.Queue(0)
+    qg = sb.createDeviceCSRGraph(queue, q)
+    dh = sb.createDeviceCSRGraph(queue, d)
+    dl = sb.createDeviceCSRGraphFromLocal(queue, d)
+    assert (dl.num_graphs, dl.total_nodes, dl.total_edges, dl.max_graph_nodes) == \
+        (dh.num_graphs, dh.total_nodes, dh.total_edges, dh.max_graph_nodes)
+    g1, g2 = sb.GMCR(queue), sb.GMCR(queue)
+    r1 = sb.match_batched(queue, qg, dh, 4, False, None, g1)
+    r2 = sb.match_batched(queue, qg, dl, 4, False, None, g2)
+    assert r1["total_matches"] == r2["total_matches"] and r1["admitted_pairs"] == r2["admitted_pairs"]
+    assert np.array_equal(g1.getPairCounts(), g2.getPairCounts())
+    # a local neighbour id outside its graph is refused
+    n, e, rows, cols = d.local_arrays()
+    cols = cols.copy()
+    cols[5] = n[0] + 7
+    import ctypes
+    from sigmo_b200 import _lib as L
+    h = ctypes.c_void_p()
+    nl, el = np.ascontiguousarray(d.node_labels), np.ascontiguousarray(d.edge_labels)
+    rc = L.lib().sigmo_graph_create_from_local(queue._h, d.num_graphs, n.ctypes.data, e.ctypes.data, rows.ctypes.data,
+                                               cols.ctypes.data, nl.ctypes.data, el.ctypes.data, ctypes.byref(h))
+    assert rc == 1 and "outside its graph" in L.last_error()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("profile,wg", [("ref-ptx", 128), ("ref-ptx", 64), ("exact", 128)])
+def test_wildcard_join_matches_oracle(profile, wg):
+    """joinWildcardCandidates (bond labels, max-candidate root, sub-group
+    split) on the plain form's final bitset and GMCR, find-all and
+    find-first, per slot against the oracle.  The batch includes the molecules
+    below vertex 256, where the reference's visited bitset is live."""
+    d = sb.generate_molecules(1200, 8, 40, seed=4601)
+    q = sb.generate_queries(30, 3, 10, seed=4602, skew_lo=4, skew_hi=8)
+    prof = {"ref-ptx": oracle.REF_PTX, "exact": oracle.EXACT}[profile]
+    queue = sb.Queue(0, profile=profile, join_work_group_size=wg)
+    qg, dg = sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)
+    cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes)
+    sig = sb.Signature(queue, dg.total_nodes, qg.total_nodes)
+    sig.generateDataSignatures(dg)
+    sig.generateQuerySignatures(qg)
+    sb.filterCandidates(queue, qg, dg, sig, cand)
+    for r in range(1, 4):
+        sig.refineDataSignatures(dg, r)
+        sig.refineQuerySignatures(qg, r)
+        sb.refineCandidates(queue, qg, dg, sig, cand)
+    gm = sb.GMCR(queue)
+    gm.generateGMCR(qg, dg, cand)
+    off, idx = gm.getGMCR()
+    bits = cand.getHostCandidates()
+    for ff in (False, True):
+        nm = np.zeros(1, np.uint64)
+        _, per = sb.isomorphism.join.joinWildcardCandidates(queue, qg, dg, cand, gm, nm, ff, per_pair=True)
+        want_total, want_per = oracle.join_wildcard(q, d, bits, off, idx, prof, ff, wg)
+        assert int(nm[0]) == want_total
+        assert np.array_equal(per, want_per)

@@ -256,3 +256,65 @@ def test_digest_is_order_sensitive():
     b3 = b.copy()
     b3[2, 3] ^= 1
     assert d0 != oracle.digest(b3)
+
+
+def _edge_label_map(b, g):
+    s, e = int(b.graph_offsets[g]), int(b.graph_offsets[g + 1])
+    lab = {}
+    for v in range(s, e):
+        for i in range(int(b.row_offsets[v]), int(b.row_offsets[v + 1])):
+            lab[(v, int(b.column_indices[i]))] = int(b.edge_labels[i])
+    return lab
+
+
+@pytest.mark.parametrize("profile", [oracle.EXACT, oracle.REF_PTX])
+def test_wildcard_join_counts_bond_labelled_embeddings(profile):
+    """joinWildcardCandidates, find-all: the root's starting candidates
+    partition the search, so the total is the number of tuples of candidates
+    with induced adjacency and equal bond labels on query edges (injective for
+    EXACT; under REF_PTX the visited set is inert for graphs starting at
+    vertex >= 256, so those graphs count non-injective tuples)."""
+    import itertools
+
+    import sigmo_b200 as sb
+
+    d = sb.generate_molecules(40, 6, 12, seed=3301)
+    q = sb.generate_queries(6, 3, 5, seed=3302)
+    qb, db = oracle.as_batch(q), oracle.as_batch(d)
+    out = oracle.run_pipeline(qb, db, 2, profile, False)
+    bits, off, idx = out["bits"], out["offsets"], out["indices"]
+    total, per = oracle.join_wildcard(qb, db, bits, off, idx, profile, False)
+    W = bits.shape[1]
+    ql_all = {}
+    for g in range(db.num_graphs):
+        s, e = int(db.graph_offsets[g]), int(db.graph_offsets[g + 1])
+        if profile == oracle.REF_PTX and s < 256:
+            continue  # the literal visited set is live there; covered by the GPU parity test
+        dlab = _edge_label_map(db, g)
+        for slot in range(int(off[g]), int(off[g + 1])):
+            qg = int(idx[slot])
+            qo, qe = int(qb.graph_offsets[qg]), int(qb.graph_offsets[qg + 1])
+            if qg not in ql_all:
+                ql_all[qg] = _edge_label_map(qb, qg)
+            qlab = ql_all[qg]
+            cands = []
+            for v in range(qo, qe):
+                row = bits[v]
+                cands.append([x for x in range(s, e) if (int(row[x >> 5]) >> (x & 31)) & 1])
+            cnt = 0
+            for tup in itertools.product(*cands):
+                if profile == oracle.EXACT and len(set(tup)) < len(tup):
+                    continue
+                ok = True
+                for i in range(qe - qo):
+                    for j in range(i + 1, qe - qo):
+                        qa = (qo + i, qo + j) in qlab
+                        da = (tup[i], tup[j]) in dlab
+                        if qa != da or (qa and qlab[(qo + i, qo + j)] != dlab[(tup[i], tup[j])]):
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                cnt += ok
+            assert per[slot] == cnt, (g, qg, per[slot], cnt)
+    assert total == int(per.sum())
