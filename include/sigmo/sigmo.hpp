@@ -163,34 +163,37 @@ struct DeviceBatchedCSRGraph {
   size_t total_edges = 0;
 };
 
-// createDeviceCSRGraph (graph.hpp:255-314): host concatenation, then upload.
+// createDeviceCSRGraph (graph.hpp:255-314).  The graphs' own arrays are
+// copied back to back (no per-element rebasing on the host) and the batch is
+// assembled on the device (sigmo_graph_create_from_local; the reference
+// concatenates on the host, graph.hpp:254).
 inline DeviceBatchedCSRGraph createDeviceCSRGraph(Queue& queue, std::vector<CSRGraph>& graphs) {
   size_t N = 0, E = 0;
   for (auto& g : graphs) {
     N += g.getNumNodes();
     E += g.getRowOffsets()[g.getNumNodes()];
   }
-  std::vector<uint32_t> go(graphs.size() + 1), ro(N + 1), col(E);
-  std::vector<uint8_t> nl(N), el(E);
-  size_t vo = 0, eo = 0;
-  go[0] = 0;
-  for (size_t gi = 0; gi < graphs.size(); ++gi) {
+  const size_t G = graphs.size();
+  std::vector<uint32_t> nc(G), ec(G), ro, col;
+  std::vector<uint8_t> nl, el;
+  ro.reserve(N + G);
+  col.reserve(E);
+  nl.reserve(N);
+  el.reserve(E);
+  for (size_t gi = 0; gi < G; ++gi) {
     auto& g = graphs[gi];
     const size_t n = g.getNumNodes(), m = g.getRowOffsets()[n];
-    go[gi + 1] = static_cast<uint32_t>(vo + n);
-    for (size_t j = 0; j <= n; ++j) ro[vo + j] = static_cast<uint32_t>(g.getRowOffsets()[j] + eo);
-    for (size_t j = 0; j < m; ++j) {
-      col[eo + j] = static_cast<uint32_t>(g.getColumnIndices()[j] + vo);
-      el[eo + j] = g.getEdgeLabels()[j];
-    }
-    for (size_t j = 0; j < n; ++j) nl[vo + j] = g.getNodeLabels()[j];
-    vo += n;
-    eo += m;
+    nc[gi] = static_cast<uint32_t>(n);
+    ec[gi] = static_cast<uint32_t>(m);
+    ro.insert(ro.end(), g.getRowOffsets(), g.getRowOffsets() + n + 1);
+    col.insert(col.end(), g.getColumnIndices(), g.getColumnIndices() + m);
+    nl.insert(nl.end(), g.getNodeLabels(), g.getNodeLabels() + n);
+    el.insert(el.end(), g.getEdgeLabels(), g.getEdgeLabels() + m);
   }
-  sigmo_host_graphs h{static_cast<uint32_t>(graphs.size()), N, E, go.data(), ro.data(), col.data(), nl.data(), el.data()};
   DeviceBatchedCSRGraph d;
-  check(sigmo_graph_create(queue.handle(), &h, &d.handle));
-  d.num_graphs = h.num_graphs;
+  check(sigmo_graph_create_from_local(queue.handle(), static_cast<uint32_t>(G), nc.data(), ec.data(), ro.data(), col.data(),
+                                      nl.data(), el.data(), &d.handle));
+  d.num_graphs = static_cast<uint32_t>(G);
   d.total_nodes = N;
   d.total_edges = E;
   return d;
@@ -375,6 +378,17 @@ inline utils::BatchedEvent joinCandidates(Queue& queue, DeviceBatchedCSRGraph& q
   uint64_t acc = *num_matches;
   check(sigmo_join_candidates(queue.handle(), query_graphs.handle, data_graphs.handle, candidates.handle(), gmcr.handle(),
                               &acc, find_first ? 1 : 0, nullptr));
+  *num_matches = static_cast<size_t>(acc);
+  return utils::BatchedEvent(queue);
+}
+
+// joinWildcardCandidates (isomorphism.hpp:435-560): bond-label-aware join.
+inline utils::BatchedEvent joinWildcardCandidates(Queue& queue, DeviceBatchedCSRGraph& query_graphs,
+                                                  DeviceBatchedCSRGraph& data_graphs, candidates::Candidates& candidates,
+                                                  mapping::GMCR& gmcr, size_t* num_matches, bool find_first = true) {
+  uint64_t acc = *num_matches;
+  check(sigmo_join_wildcard_candidates(queue.handle(), query_graphs.handle, data_graphs.handle, candidates.handle(),
+                                       gmcr.handle(), &acc, find_first ? 1 : 0, nullptr));
   *num_matches = static_cast<size_t>(acc);
   return utils::BatchedEvent(queue);
 }

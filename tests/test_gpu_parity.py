@@ -304,3 +304,28 @@ def test_wildcard_join_matches_oracle(profile, wg):
         want_total, want_per = oracle.join_wildcard(q, d, bits, off, idx, prof, ff, wg)
         assert int(nm[0]) == want_total
         assert np.array_equal(per, want_per)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("extra", [[], ["--batched"]])
+def test_cli_driver_matches_oracle(tmp_path, extra):
+    """The reference driver rewritten on the C++ API (sigmo_b200/sigmo_cli):
+    text files in, '# Matches' out, as SIGMo's log parser reads it."""
+    import subprocess
+    from pathlib import Path
+
+    d = sb.generate_molecules(800, 10, 40, seed=4701)
+    q = sb.generate_queries(25, 3, 10, seed=4702)
+    (tmp_path / "d.dat").write_text(d.to_text())
+    (tmp_path / "q.dat").write_text(q.to_text())
+    cli = Path(sb.__file__).resolve().parent / "sigmo_cli"
+    for find_all in (True, False):
+        cmd = [str(cli), "-Q", str(tmp_path / "q.dat"), "-D", str(tmp_path / "d.dat"), "-i", "3", "--skip-candidates-analysis",
+               "--max-data-graphs", "1000000", "--max-query-graphs", "1000000"] + (["--find-all"] if find_all else []) + extra
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        line = [l for l in out.stdout.splitlines() if l.startswith("# Matches:")][0]
+        got = int(line.split(":")[1].strip().replace(".", ""))
+        qb, db = oracle.parse_text(q.to_text()), oracle.parse_text(d.to_text())
+        want = oracle.run_pipeline(qb, db, 3, oracle.REF_PTX, not find_all)["total"]
+        assert got == want, (find_all, extra, got, want)
