@@ -118,13 +118,16 @@ SIGMO_API void sigmo_default_options(sigmo_options* o);
 
 /* Launch shape of the batched join (no reference counterpart; the
  * reference's only knob is the join work-group size above).  Zero fields take
- * the defaults.  sigmo_autotune searches these on a caller's own workload. */
+ * the defaults (overflow_serial: 0 is a value, run beside).  sigmo_autotune
+ * searches these on a caller's own workload. */
 typedef struct sigmo_tuning {
   uint32_t join_blocks_per_sm;   /* persistent join CTAs per SM, 1..3 (3)                      */
   uint32_t join_chunk;           /* GMCR slots a lane takes per work grab, 1..64 (4)             */
   uint32_t overflow_blocks;      /* CTAs of the join for queries over 16 vertices (1184)        */
-  uint32_t overflow_serial;      /* 1: run those after the main join instead of beside it (0)   */
+  uint32_t overflow_serial;      /* 1 (default): run those after the main join; 0: beside it      */
   uint32_t mask_chunk_slots;     /* GMCR slots per level-mask pass, in 2^20 units, 1..64 (8)     */
+  uint32_t overflow_split;       /* work items per pair of those queries, each taking every
+                                    split-th root candidate, 1..64 (16)                          */
 } sigmo_tuning;
 /* sycl::queue{gpu_selector_v, enable_profiling} (library/src/sigmo.cpp:19). */
 SIGMO_API int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out);

@@ -51,6 +51,7 @@ class TuningC(ctypes.Structure):
         ("overflow_blocks", ctypes.c_uint32),
         ("overflow_serial", ctypes.c_uint32),
         ("mask_chunk_slots", ctypes.c_uint32),
+        ("overflow_split", ctypes.c_uint32),
     ]
 
 

@@ -429,7 +429,8 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   SIGMO_CUDA_TRY(cudaSetDevice(q->device));
   const sigmo_tuning& tn = q->tune;
   const uint64_t key[6] = {query->stamp, data->stamp, R, static_cast<uint64_t>(find_first),
-                           static_cast<uint64_t>(q->opts.profile) | (static_cast<uint64_t>(tn.overflow_serial) << 8),
+                           static_cast<uint64_t>(q->opts.profile) | (static_cast<uint64_t>(tn.overflow_serial) << 8) |
+                               (static_cast<uint64_t>(tn.overflow_split) << 16),
                            (static_cast<uint64_t>(tn.join_blocks_per_sm) << 48) | (static_cast<uint64_t>(tn.join_chunk) << 40) |
                                (static_cast<uint64_t>(tn.mask_chunk_slots) << 32) | tn.overflow_blocks};
   if (graph && !materialize && m->graph && std::equal(key, key + 6, m->graph_key)) {
@@ -525,8 +526,7 @@ extern "C" int sigmo_autotune(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_
     *total = r.total_matches;
     return SIGMO_OK;
   };
-  sigmo_tuning cur{};
-  normalize_tuning(&cur);
+  sigmo_tuning cur = Queue{}.tune;  // the library default
   double cur_ms = 0, d_ms = 0;
   uint64_t d_total = 0, total = 0;
   int rc = measure(cur, &d_ms, &d_total);
@@ -541,6 +541,7 @@ extern "C" int sigmo_autotune(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_
       {&sigmo_tuning::join_chunk, {1, 2, 4, 8, 16}},
       {&sigmo_tuning::overflow_blocks, {148, 296, 592, 1184, 2368}},
       {&sigmo_tuning::mask_chunk_slots, {2, 8, 32}},
+      {&sigmo_tuning::overflow_split, {1, 4, 16, 32}},
   };
   for (const Axis& ax : axes) {
     for (uint32_t v : ax.values) {

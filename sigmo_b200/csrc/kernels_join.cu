@@ -484,10 +484,13 @@ __global__ void __launch_bounds__(128) k_join_fast(
     const uint8_t* __restrict__ qsym, const uint32_t* __restrict__ dgoff, const uint64_t* __restrict__ dadj,
     const uint8_t* __restrict__ dsym, const uint32_t* __restrict__ indices, const uint32_t* __restrict__ pair_graph,
     const uint32_t* __restrict__ list, const unsigned long long* __restrict__ list_len, uint64_t total_slots,
-    uint32_t skip_below, int find_first, unsigned long long* __restrict__ cursor, uint64_t* __restrict__ counts,
-    unsigned long long* __restrict__ d_total) {
+    uint32_t skip_below, int find_first, uint32_t split, unsigned long long* __restrict__ cursor,
+    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total) {
   constexpr uint32_t kChunk = 8;
-  const uint64_t total = list ? *list_len : total_slots;  // entries to walk (list or all slots)
+  // entries to walk (list or all slots); with split > 1 every entry is split
+  // into `split` work items, item p taking the root candidates of rank = p mod
+  // split, and the items' counts are merged into counts[] (zeroed beforehand)
+  const uint64_t total = (list ? *list_len : total_slots) * split;
   const unsigned lane = threadIdx.x & 31u;
   uint64_t my_total = 0;
   uint64_t M[kMaxQueryNodes][AW];     // candidates of each level (graph-local)
@@ -496,6 +499,7 @@ __global__ void __launch_bounds__(128) k_join_fast(
   uint32_t pick[kMaxQueryNodes];
   uint64_t next = 0, end = 0;  // this lane's claimed slot range
   uint64_t slot = 0;
+  uint32_t part = 0;
   uint64_t cnt = 0;
   uint32_t n = 0, s = 0;
   const uint64_t* selp = nullptr;
@@ -505,8 +509,17 @@ __global__ void __launch_bounds__(128) k_join_fast(
     if (k < 0) {
       if (have) {
         if (find_first && cnt) cnt = 1;
-        counts[slot] = cnt;
-        my_total += cnt;
+        if (split == 1) {
+          counts[slot] = cnt;
+          my_total += cnt;
+        } else if (cnt) {
+          if (!find_first) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(counts + slot), static_cast<unsigned long long>(cnt));
+            my_total += cnt;
+          } else if (atomicCAS(reinterpret_cast<unsigned long long*>(counts + slot), 0ull, 1ull) == 0ull) {
+            my_total += 1;
+          }
+        }
         have = false;
       }
       // claim the next slot of a pair this kernel handles
@@ -526,7 +539,9 @@ __global__ void __launch_bounds__(128) k_join_fast(
             break;
           }
         }
-        slot = list ? list[next] : next;
+        const uint64_t entry = next / split;
+        part = static_cast<uint32_t>(next % split);
+        slot = list ? list[entry] : entry;
         ++next;
         if (pair_graph[slot] >= skip_below) break;
       }
@@ -546,6 +561,20 @@ __global__ void __launch_bounds__(128) k_join_fast(
       }
 #pragma unroll
       for (int w = 0; w < AW; ++w) cand[0][w] = M[0][w];
+      if (split > 1) {  // keep the root candidates of rank = part mod split
+        uint32_t rank = 0;
+#pragma unroll
+        for (int w = 0; w < AW; ++w) {
+          uint64_t bitsw = cand[0][w], keep = 0;
+          while (bitsw) {
+            const uint64_t low = bitsw & (0ull - bitsw);
+            if (rank % split == part) keep |= low;
+            ++rank;
+            bitsw ^= low;
+          }
+          cand[0][w] = keep;
+        }
+      }
       cnt = 0;
       k = 0;
       have = true;
@@ -623,7 +652,7 @@ __global__ void __launch_bounds__(256) k_pair_masks(
     const uint8_t* __restrict__ qsym, const uint32_t* __restrict__ dgoff, const uint8_t* __restrict__ dsym,
     const uint32_t* __restrict__ indices, const uint32_t* __restrict__ pair_graph, uint64_t slot0, uint64_t count,
     uint64_t* __restrict__ masks, uint4* __restrict__ rec, uint32_t skip_below, uint32_t* __restrict__ overflow,
-    unsigned long long* __restrict__ overflow_len) {
+    unsigned long long* __restrict__ overflow_len, uint64_t* __restrict__ counts) {
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count * kPhaseLevels; i += stride) {
     const uint64_t local = i % count;  // slot within the chunk (fastest), then level
@@ -636,7 +665,10 @@ __global__ void __launch_bounds__(256) k_pair_masks(
     const bool ident = !(qsym[qg] && dsym[g]);
     if (j == 0) {  // the pair's setup record: first data vertex, query size, query offset, order
       rec[local] = make_uint4(dgoff[g], n | (ident ? 0x100u : 0u), qoff, g);
-      if (n > kPhaseLevels && g >= skip_below) overflow[atomicAdd(overflow_len, 1ull)] = static_cast<uint32_t>(slot);
+      if (n > kPhaseLevels && g >= skip_below) {  // joined by the generic kernel, which accumulates into counts
+        overflow[atomicAdd(overflow_len, 1ull)] = static_cast<uint32_t>(slot);
+        counts[slot] = 0;
+      }
     }
     if (n > kPhaseLevels) continue;
     const uint32_t c = cls[qoff + (ident ? j : qorder[qoff + j])];
@@ -810,7 +842,7 @@ int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Cand
                                                        q->opts.profile, query->graph_offsets, query->qorder,             \
                                                        query->qsel, query->qsel_id, query->sym, data->graph_offsets,     \
                                                        data->adj, data->sym, m->indices, m->pair_graph, nullptr, nullptr, \
-                                                       m->total, skip, find_first, cursor, m->counts, tot)
+                                                       m->total, skip, find_first, 1u, cursor, m->counts, tot)
   switch (data->adj_words) {
     case 1: if (exact) SIGMO_JOIN_FAST(1, true); else SIGMO_JOIN_FAST(1, false); break;
     case 2: if (exact) SIGMO_JOIN_FAST(2, true); else SIGMO_JOIN_FAST(2, false); break;
@@ -852,7 +884,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
       auto* recs = reinterpret_cast<uint4*>(masks + kPhaseLevels * chunk);
       k_pair_masks<<<grid_for(cnt * kPhaseLevels, 256, 148u * 32u), 256, 0, q->stream>>>(
           planes, planes_rows, pp.prog_off, prog, pp.cls, query->graph_offsets, query->qorder, query->sym, data->graph_offsets,
-          data->sym, m->indices, m->pair_graph, slot0, cnt, masks, recs, skip, overflow, ctr + 2);
+          data->sym, m->indices, m->pair_graph, slot0, cnt, masks, recs, skip, overflow, ctr + 2, m->counts);
       rc = check_launch(q, "k_pair_masks");
       if (!rc && slot0 + chunk >= m->total && cudaEventRecord(q->ev_fork, q->stream) != cudaSuccess)
         rc = fail(SIGMO_ERR_CUDA, "event record failed");
@@ -887,13 +919,15 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
     const unsigned block = 128;
     const unsigned grid = tiles ? q->tune.overflow_blocks : 148u * 8u;
     const uint32_t* list = tiles ? overflow : nullptr;
+    const uint32_t split = tiles ? q->tune.overflow_split : 1u;
     const unsigned long long* list_len = tiles ? ctr + 2 : nullptr;
 #define SIGMO_JOIN_PLANES(AWV, EX)                                                                                      \
   k_join_fast<AWV, EX, true><<<grid, block, 0, q->stream>>>(nullptr, 0, planes, planes_rows, pp.prog_off, prog, pp.cls,  \
                                                             q->opts.profile, query->graph_offsets, query->qorder,        \
                                                             query->qsel, query->qsel_id, query->sym, data->graph_offsets, \
                                                             data->adj, data->sym, m->indices, m->pair_graph, list,       \
-                                                            list_len, m->total, skip, find_first, ctr + 1, m->counts, tot)
+                                                            list_len, m->total, skip, find_first, split, ctr + 1, m->counts, \
+                                                            tot)
     switch (data->adj_words) {
       case 1: if (exact) SIGMO_JOIN_PLANES(1, true); else SIGMO_JOIN_PLANES(1, false); break;
       case 2: if (exact) SIGMO_JOIN_PLANES(2, true); else SIGMO_JOIN_PLANES(2, false); break;

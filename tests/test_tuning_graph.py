@@ -50,18 +50,23 @@ def test_autotune_keeps_results_and_sets_the_queue():
     queue = sb.Queue(0)
     q, d, qg, dg = _graphs(queue, 4000, 80, 1721)
     base = sb.match_batched(queue, qg, dg, R, False, None, sb.GMCR(queue))
+    base_ff = sb.match_batched(queue, qg, dg, R, True, None, sb.GMCR(queue))
     t = sb.autotune(queue, qg, dg, R, False, reps=1)
     assert t["ms_join"] > 0 and t["ms_join_default"] > 0
     assert t["ms_join"] <= t["ms_join_default"] * 1.05
     got = queue.get_tuning()
-    for k in ("join_blocks_per_sm", "join_chunk", "overflow_blocks", "overflow_serial", "mask_chunk_slots"):
+    for k in ("join_blocks_per_sm", "join_chunk", "overflow_blocks", "overflow_serial", "mask_chunk_slots", "overflow_split"):
         assert got[k] == t[k]
     after = sb.match_batched(queue, qg, dg, R, False, None, sb.GMCR(queue))
     assert after["total_matches"] == base["total_matches"]
     # explicit shapes, including the serial overflow path and small mask chunks
-    queue.set_tuning(join_blocks_per_sm=1, join_chunk=16, overflow_blocks=148, overflow_serial=1, mask_chunk_slots=1)
-    gm = sb.GMCR(queue)
-    r = sb.match_batched(queue, qg, dg, R, False, None, gm)
-    assert r["total_matches"] == base["total_matches"]
+    for split in (1, 3, 32):
+        queue.set_tuning(join_blocks_per_sm=1, join_chunk=16, overflow_blocks=148, overflow_serial=1, mask_chunk_slots=1,
+                         overflow_split=split)
+        gm = sb.GMCR(queue)
+        r = sb.match_batched(queue, qg, dg, R, False, None, gm)
+        assert r["total_matches"] == base["total_matches"]
+        f = sb.match_batched(queue, qg, dg, R, True, None, gm)
+        assert f["total_matches"] == base_ff["total_matches"]
     with pytest.raises(sb.SigmoError):
         queue.set_tuning(join_blocks_per_sm=9)
