@@ -7,7 +7,6 @@
 
 #include <algorithm>
 #include <cstring>
-#include <map>
 #include <vector>
 
 #include "internal.hpp"
@@ -56,65 +55,84 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   }
   SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));
 
-  // planes: label values used by queries, then thresholds (r, l, c)
-  std::map<uint32_t, uint32_t> label_plane;
-  std::map<uint32_t, uint32_t> ge_plane;  // key r<<16 | l<<8 | c
-  for (uint64_t v = 0; v < Qn; ++v) label_plane[lab[v]] = 0;
-  for (uint32_t r = 0; r < R; ++r)
-    for (uint64_t v = 0; v < Qn; ++v) {
-      const uint64_t s = sig[r * Qn + v];
-      for (uint32_t l = 0; l < 16; ++l) {
-        const uint32_t c = sig_get(s, l);
-        if (c) ge_plane[(r << 16) | (l << 8) | c] = 0;
-      }
+  // planes: label values used by queries (ascending), then the thresholds
+  // (r, l, c) that occur, in (r, l, c) order
+  std::vector<uint8_t> label_used(256, 0);
+  for (uint64_t v = 0; v < Qn; ++v) label_used[lab[v]] = 1;
+  std::vector<uint8_t> thr_used(static_cast<size_t>(R) * 16 * 16, 0);  // [r][l][c]
+  // non-zero counters only: bit 4l of the nibble mask is set when counter l is
+  auto for_counters = [](uint64_t sv, auto&& f) {
+    for (uint64_t nz = sig_nonzero_nibbles(sv); nz; nz &= nz - 1) {
+      const uint32_t l = static_cast<uint32_t>(__builtin_ctzll(nz)) >> 2;
+      f(l, static_cast<uint32_t>((sv >> (4 * l)) & 0xFu));
     }
+  };
+  for (uint32_t r = 0; r < R; ++r)
+    for (uint64_t v = 0; v < Qn; ++v)
+      for_counters(sig[r * Qn + v], [&](uint32_t l, uint32_t c) { thr_used[(r * 16 + l) * 16 + c] = 1; });
   std::vector<uint32_t> spec;
-  for (auto& kv : label_plane) {
-    kv.second = static_cast<uint32_t>(spec.size());
-    spec.push_back(0x80000000u | kv.first);
-  }
-  for (auto& kv : ge_plane) {
-    kv.second = static_cast<uint32_t>(spec.size());
-    spec.push_back(kv.first);
-  }
+  std::vector<uint32_t> label_idx(256, 0), thr_idx(thr_used.size(), 0);
+  for (uint32_t l = 0; l < 256; ++l)
+    if (label_used[l]) {
+      label_idx[l] = static_cast<uint32_t>(spec.size());
+      spec.push_back(0x80000000u | l);
+    }
+  const uint32_t nlab = static_cast<uint32_t>(spec.size());
+  for (uint32_t r = 0; r < R; ++r)
+    for (uint32_t l = 0; l < 16; ++l)
+      for (uint32_t c = 1; c < 16; ++c)
+        if (thr_used[(r * 16 + l) * 16 + c]) {
+          thr_idx[(r * 16 + l) * 16 + c] = static_cast<uint32_t>(spec.size());
+          spec.push_back((r << 16) | (l << 8) | c);
+        }
   if (spec.size() >= 65535) return fail(SIGMO_ERR_DOMAIN, "query batch needs %zu candidate planes (limit 65535)", spec.size());
 
   // classes: distinct (label, sig_1..sig_R); program = label plane, then the
-  // thresholds in (r, l) order; classes numbered in lexicographic program order.
-  std::map<std::vector<uint16_t>, uint32_t> programs;  // program -> class
-  std::vector<uint16_t> cur;
-  std::vector<std::vector<uint16_t>> prog_of_vertex(Qn);
+  // thresholds in (r, l) order; classes numbered in lexicographic program
+  // order (one sort of the vertices by program).
+  std::vector<uint32_t> voff(Qn + 1, 0);
+  std::vector<uint16_t> vprog;
+  vprog.reserve(Qn * 8);
   for (uint64_t v = 0; v < Qn; ++v) {
-    cur.clear();
-    cur.push_back(static_cast<uint16_t>(label_plane[lab[v]]));
+    vprog.push_back(static_cast<uint16_t>(label_idx[lab[v]]));
     for (uint32_t r = 0; r < R; ++r)
-      for (uint32_t l = 0; l < 16; ++l) {
-        const uint32_t c = sig_get(sig[r * Qn + v], l);
-        if (c) cur.push_back(static_cast<uint16_t>(ge_plane[(r << 16) | (l << 8) | c]));
-      }
-    programs.emplace(cur, 0u);
-    prog_of_vertex[v] = cur;
+      for_counters(sig[r * Qn + v],
+                   [&](uint32_t l, uint32_t c) { vprog.push_back(static_cast<uint16_t>(thr_idx[(r * 16 + l) * 16 + c])); });
+    voff[v + 1] = static_cast<uint32_t>(vprog.size());
   }
+  auto prog_less = [&](uint32_t a, uint32_t b2) {
+    return std::lexicographical_compare(vprog.begin() + voff[a], vprog.begin() + voff[a + 1], vprog.begin() + voff[b2],
+                                        vprog.begin() + voff[b2 + 1]);
+  };
+  auto prog_equal = [&](uint32_t a, uint32_t b2) {
+    return voff[a + 1] - voff[a] == voff[b2 + 1] - voff[b2] &&
+           std::equal(vprog.begin() + voff[a], vprog.begin() + voff[a + 1], vprog.begin() + voff[b2]);
+  };
+  std::vector<uint32_t> by_prog(Qn);
+  for (uint64_t v = 0; v < Qn; ++v) by_prog[v] = static_cast<uint32_t>(v);
+  std::sort(by_prog.begin(), by_prog.end(), prog_less);
   std::vector<uint32_t> cls(Qn), prog_off{0};
   std::vector<uint16_t> prog;
   uint32_t max_len = 0;
-  for (auto& kv : programs) {
-    kv.second = static_cast<uint32_t>(prog_off.size() - 1);
-    prog.insert(prog.end(), kv.first.begin(), kv.first.end());
-    prog_off.push_back(static_cast<uint32_t>(prog.size()));
-    max_len = std::max<uint32_t>(max_len, static_cast<uint32_t>(kv.first.size()));
+  for (uint64_t i = 0; i < Qn; ++i) {
+    const uint32_t v = by_prog[i];
+    if (i == 0 || !prog_equal(by_prog[i - 1], v)) {
+      prog.insert(prog.end(), vprog.begin() + voff[v], vprog.begin() + voff[v + 1]);
+      prog_off.push_back(static_cast<uint32_t>(prog.size()));
+      max_len = std::max<uint32_t>(max_len, voff[v + 1] - voff[v]);
+    }
+    cls[v] = static_cast<uint32_t>(prog_off.size() - 2);
   }
-  for (uint64_t v = 0; v < Qn; ++v) cls[v] = programs[prog_of_vertex[v]];
   const uint32_t C = static_cast<uint32_t>(prog_off.size() - 1);
   std::vector<uint32_t> r_begin(R + 1, static_cast<uint32_t>(spec.size()));
-  for (uint32_t k = static_cast<uint32_t>(label_plane.size()); k < spec.size(); ++k) {
+  for (uint32_t k = nlab; k < spec.size(); ++k) {
     const uint32_t r = (spec[k] >> 16) & 0xFFu;
     r_begin[r] = std::min(r_begin[r], k);
   }
   for (int r = static_cast<int>(R) - 1; r >= 0; --r) r_begin[r] = std::min(r_begin[r], r_begin[r + 1]);
   pp.K = static_cast<uint32_t>(spec.size());
   pp.C = C;
-  pp.nlab = static_cast<uint32_t>(label_plane.size());
+  pp.nlab = nlab;
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.spec), spec.data(), 4 * spec.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog_off), prog_off.data(), 4 * prog_off.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.prog), prog.data(), 2 * prog.size()));
