@@ -47,6 +47,16 @@ WORKLOADS = {
         desc="100,000 synthetic molecules (10-60 atoms) x 600 queries (3-30 atoms, skewed 6-15), 6 refinement iterations",
         mols=100_000, min_atoms=10, max_atoms=60, kind=0, median=22.0, queries=600, qmin=3, qmax=30, skew=(6, 15),
         qkind=0, R=6, seed_d=20251, seed_q=20252),
+    "uneven1m": dict(
+        desc="1,000,000 synthetic molecules (6-120 atoms, lognormal median 22, 5% macrocycles / fused systems) x 2,000 "
+             "queries (3-40 atoms), 6 refinement iterations",
+        mols=1_000_000, min_atoms=6, max_atoms=120, kind=1, median=22.0, queries=2000, qmin=3, qmax=40, skew=(0, 0),
+        qkind=0, R=6, seed_d=30301, seed_q=30302),
+    "symmetry2m": dict(
+        desc="2,000,000 ring-rich synthetic molecules (2-6 fused aromatic 6-cycles, carbon chains up to 20) x 300 highly "
+             "automorphic queries (6-cycles, fused bi/tri-cycles, carbon chains 4-12, branched stars), 6 refinement iterations",
+        mols=2_000_000, min_atoms=10, max_atoms=64, kind=2, median=22.0, queries=300, qmin=4, qmax=14, skew=(0, 0),
+        qkind=3, R=6, seed_d=50501, seed_q=50502),
     "drug1k": dict(
         desc="1,000 synthetic molecules (10-40 atoms) x 20 queries (4-12 atoms), 6 refinement iterations",
         mols=1_000, min_atoms=10, max_atoms=40, kind=0, median=22.0, queries=20, qmin=4, qmax=12, skew=(0, 0),
@@ -200,13 +210,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_for(kernel: str, workload: str):
+def traffic_for(kernel: str, workload: str, key: str = "bytes_per_launch"):
+    """A per-launch figure of one ncu capture summarised under profiles/."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
     j = json.loads(p.read_text())
     e = j.get(f"{kernel}@{workload}")
-    return None if e is None else e.get("bytes_per_launch")
+    return None if e is None else e.get(key)
 
 
 def join_bytes(q, d, offsets, indices):
@@ -396,7 +407,10 @@ def run_sigmo(args, rank, world, local):
             "frac": round(achieved / hbm, 4), "traffic": traffic_for("join", args.workload),
             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured" else peak_kind,
             "algorithmic_bytes_per_launch": jb, "ms_per_launch": round(join_ms, 4),
-            "note": "DFS over admitted pairs: latency/issue-bound, no bandwidth roofline applies; the stage is "
+            "warp_execution_efficiency": traffic_for("join", args.workload, "warp_execution_efficiency"),
+            "active_warps_of_peak": traffic_for("join", args.workload, "active_warps_of_peak"),
+            "note": "DFS over admitted pairs: latency/issue-bound, no bandwidth roofline applies (ncu: threads per "
+                    "instruction / 32 and active warps above); the stage is "
                     f"{100 * join_ms / stages['ms_total']:.0f}% of the step"}
 
     # ---- the plain stage-per-launch form (same results, reference order) ----
