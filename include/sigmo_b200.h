@@ -170,6 +170,15 @@ SIGMO_API int sigmo_graph_create_from_local(sigmo_queue_t q, uint32_t num_graphs
                                             const uint32_t* edge_counts, const uint32_t* row_offsets_local,
                                             const uint32_t* columns_local, const uint8_t* node_labels,
                                             const uint8_t* edge_labels, sigmo_graph_t* out);
+/* Marks a data batch as a shard of a larger one whose vertex 0 has global id
+ * `base` (no reference counterpart; the reference's MPI ranks restart ids at
+ * 0, sigmo_mpi.cpp:114,126).  REF_PTX results depend on global ids (the
+ * range-mask rule at 32-vertex words, the live `visited` bitset below vertex
+ * 256), so a shard keeps the semantics of the unsharded batch.  base must be
+ * 0 or >= 256 (the graphs starting below vertex 256 stay in the first shard);
+ * sigmo_match_batched then gives the shard's part of the unsharded GMCR and
+ * counts.  Used by the batched form's planes route only. */
+SIGMO_API int sigmo_graph_set_vertex_base(sigmo_graph_t g, uint32_t base);
 /* destroyDeviceCSRGraph (graph.hpp:316-322). */
 SIGMO_API int sigmo_graph_destroy(sigmo_graph_t g);
 SIGMO_API int sigmo_graph_info(sigmo_graph_t g, uint32_t* num_graphs, uint64_t* total_nodes, uint64_t* total_edges,

@@ -283,6 +283,11 @@ class DeviceBatchedCSRGraph:
         except Exception:
             pass
 
+    def set_vertex_base(self, base: int) -> None:
+        """This batch is a shard whose vertex 0 has global id `base`
+        (sigmo_graph_set_vertex_base)."""
+        check(lib().sigmo_graph_set_vertex_base(self._h, base))
+
     def alloc_size(self) -> int:
         v = ctypes.c_uint64()
         check(lib().sigmo_graph_alloc_size(self._h, ctypes.byref(v)))
@@ -560,6 +565,39 @@ def autotune(queue: Queue, query_graphs, data_graphs, iterations: int, find_firs
     out = {f: getattr(t, f) for f, _ in _L.TuningC._fields_}
     out.update(ms_join=best.value, ms_join_default=default.value)
     return out
+
+
+# ---- sharding ---------------------------------------------------------------------
+def shard_plan(graphs: HostGraphs, shards: int, weight=None, min_first: int = 256):
+    """Contiguous ranges of data graphs, one per shard, balanced by `weight`
+    per graph (default: vertices).  The first shard ends at or after global
+    vertex `min_first`, so every later shard starts at a global id the
+    sharded semantics allow.  Returns [(first_graph, count, vertex_base)]."""
+    sizes = graphs.sizes()
+    w = sizes.astype(np.float64) if weight is None else np.asarray(weight, np.float64)
+    goff = graphs.graph_offsets.astype(np.int64)
+    G = len(sizes)
+    cum = np.concatenate([[0.0], np.cumsum(w)])
+    bounds = [0]
+    for s in range(1, shards):
+        b = int(np.searchsorted(cum, cum[-1] * s / shards))
+        b = max(b, bounds[-1])
+        if s == 1:
+            b = max(b, int(np.searchsorted(goff, min_first)))  # first shard covers vertex min_first
+        bounds.append(min(b, G))
+    bounds.append(G)
+    return [(bounds[i], bounds[i + 1] - bounds[i], int(goff[bounds[i]])) for i in range(shards)]
+
+
+def createDeviceShard(queue: Queue, graphs: HostGraphs, first: int, count: int) -> DeviceBatchedCSRGraph:
+    """Graphs [first, first+count) of a batch on the device, keeping the
+    global ids of the whole batch for the semantics (vertex base)."""
+    part = graphs.slice(first, count)
+    dg = createDeviceCSRGraph(queue, part)
+    base = int(graphs.graph_offsets[first]) if count else 0
+    if base:
+        dg.set_vertex_base(base)
+    return dg
 
 
 # ---- serving loop -----------------------------------------------------------------

@@ -119,6 +119,7 @@ SIGNATURES = {
     "sigmo_graphs_save": (_i, [_P(HostGraphsC), ctypes.c_char_p]),
     "sigmo_graphs_load": (_i, [ctypes.c_char_p, _P(HostGraphsC)]),
     "sigmo_graph_create_from_local": (_i, [_vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _P(_vp)]),
+    "sigmo_graph_set_vertex_base": (_i, [_vp, _u32]),
     "sigmo_generate_molecules": (_i, [_i, _u32, _u32, _u32, _d, _u64, _P(HostGraphsC)]),
     "sigmo_generate_queries": (_i, [_i, _u32, _u32, _u32, _u32, _u32, _u64, _P(HostGraphsC)]),
     "sigmo_default_options": (None, [_P(OptionsC)]),

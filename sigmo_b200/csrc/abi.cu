@@ -330,6 +330,20 @@ int sigmo_graph_create_device(sigmo_queue_t q, uint32_t num_graphs, uint64_t tot
   return SIGMO_OK;
 }
 
+int sigmo_graph_set_vertex_base(sigmo_graph_t g, uint32_t base) {
+  if (!g) return fail(SIGMO_ERR_INVALID, "null graph");
+  if (base != 0 && base < kLowOffsetLimit)
+    return fail(SIGMO_ERR_DOMAIN, "a shard must start at global vertex 0 or at %u or above (got %u)", kLowOffsetLimit, base);
+  if (static_cast<uint64_t>(base) + g->total_nodes > 0xFFFFFFFFull)
+    return fail(SIGMO_ERR_DOMAIN, "base + vertices exceeds 2^32");
+  g->vertex_base = base;
+  uint32_t low = 0;
+  for (uint32_t i = 0; i < g->num_graphs; ++i)
+    if (static_cast<uint64_t>(g->host_graph_offsets[i]) + base < kLowOffsetLimit) low = i + 1;
+  g->low_offset_graphs = low;
+  return SIGMO_OK;
+}
+
 int sigmo_graph_destroy(sigmo_graph_t g) {
   if (!g) return SIGMO_OK;
   Queue* q = g->q;

@@ -466,6 +466,9 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   int rc = cudaMemsetAsync(d_total, 0, 8, q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "memset failed");
   const bool planes_fit = planes_admit_smem(query->pp.K, data->adj_words, query->pp.C) <= 200u * 1024u;
   const bool bitset_route = materialize || !planes_fit;
+  if (!rc && bitset_route && data->vertex_base)
+    rc = fail(SIGMO_ERR_DOMAIN, "a shard (vertex base %u) runs on the planes route only; this batch needs the bitset route",
+              data->vertex_base);
   if (!rc) {
     if (bitset_route) {
       sigmo_candidates_t cc = static_cast<sigmo_candidates_t>(c);

@@ -88,6 +88,7 @@ struct Graph {
   uint64_t* adj = nullptr;         // [total_nodes * adj_words] local neighbour sets
   uint8_t* sym = nullptr;          // [num_graphs] 1 if the adjacency is mirrored
   uint32_t low_offset_graphs = 0;  // graphs whose first vertex is < 256
+  uint32_t vertex_base = 0;        // global id of vertex 0 when the batch is a shard of a larger one
   // Query-side matching orders (built on first use by the batched join):
   uint8_t* qorder = nullptr;       // [total_nodes] local id placed at level k
   uint64_t* qsel = nullptr;        // [total_nodes] adjacency to earlier levels

@@ -38,7 +38,7 @@ template <int AW>
 __device__ __forceinline__ void build_graph_planes(uint64_t* tile, uint32_t gl, uint32_t s, uint32_t e, unsigned lane,
                                                    const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
                                                    uint64_t N, uint32_t R, uint32_t nlab, const uint32_t* __restrict__ spec,
-                                                   const uint32_t* __restrict__ r_begin, int prof) {
+                                                   const uint32_t* __restrict__ r_begin, int prof, uint32_t base) {
   constexpr int P = 2 * AW;  // 32-vertex chunks per graph
   const uint32_t n = e - s;
   const uint32_t chunks = (n + 31u) / 32u;
@@ -50,7 +50,10 @@ __device__ __forceinline__ void build_graph_planes(uint64_t* tile, uint32_t gl, 
     const bool in = t < n;
     const uint32_t v = s + t;
     lb[p] = in ? lab[v] : 0;
-    vis[p] = in && ((range_mask(v >> 5, s, e, prof) >> (v & 31u)) & 1u);
+    // visibility follows global ids (base + local id): the range-mask rule
+    // depends on where the graph ends relative to 32-vertex words
+    const uint32_t gv = base + v;
+    vis[p] = in && ((range_mask(gv >> 5, base + s, base + e, prof) >> (gv & 31u)) & 1u);
   }
   auto put = [&](uint32_t k, const uint32_t (&chunk)[P]) {
 #pragma unroll
@@ -113,8 +116,9 @@ template <int AW, bool GATHER>
 __device__ __forceinline__ void fill_tile(uint64_t* tile, uint32_t gw, uint32_t G, const uint32_t* __restrict__ goff,
                                           const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all, uint64_t N,
                                           uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec,
-                                          const uint32_t* __restrict__ r_begin, int prof, const uint64_t* __restrict__ rplanes,
-                                          uint32_t rrows, const uint32_t* __restrict__ row_map) {
+                                          const uint32_t* __restrict__ r_begin, int prof, uint32_t base,
+                                          const uint64_t* __restrict__ rplanes, uint32_t rrows,
+                                          const uint32_t* __restrict__ row_map) {
   constexpr uint32_t kRow = AW * 32u;
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (GATHER) {
@@ -128,7 +132,7 @@ __device__ __forceinline__ void fill_tile(uint64_t* tile, uint32_t gw, uint32_t 
     for (uint32_t gl = wid; gl < 32; gl += nw) {
       const uint32_t g = gw * 32u + gl;
       if (g < G) {
-        build_graph_planes<AW>(tile, gl, goff[g], goff[g + 1], lane, lab, sig_all, N, R, nlab, spec, r_begin, prof);
+        build_graph_planes<AW>(tile, gl, goff[g], goff[g + 1], lane, lab, sig_all, N, R, nlab, spec, r_begin, prof, base);
       } else {
         for (uint32_t i = lane; i < K * AW; i += 32) tile[i * 32 + gl] = 0;
       }
@@ -186,7 +190,8 @@ template <int AW, bool GATHER>
 __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     uint32_t G, const uint32_t* __restrict__ goff, const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
     uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
-    int prof, const uint64_t* __restrict__ rplanes, uint32_t rrows, const uint32_t* __restrict__ row_map, uint32_t QG,
+    int prof, uint32_t base, const uint64_t* __restrict__ rplanes, uint32_t rrows, const uint32_t* __restrict__ row_map,
+    uint32_t QG,
     const uint32_t* __restrict__ qgoff, uint32_t C, const uint32_t* __restrict__ g_prog_off, const uint16_t* __restrict__ g_prog,
     const uint32_t* __restrict__ g_qc_off, const uint32_t* __restrict__ g_qc, uint32_t n_qc, uint32_t n_prog, int stage_lists,
     uint64_t* __restrict__ planes, uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
@@ -233,7 +238,7 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
       if (next < GW) gather_tile_async<AW>(tiles + static_cast<size_t>(buf ^ 1u) * words * 32, rplanes, rrows, next, K, s_map);
     } else {
       __syncthreads();  // the previous tile is no longer read
-      fill_tile<AW, false>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, nullptr, 0, nullptr);
+      fill_tile<AW, false>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, base, nullptr, 0, nullptr);
     }
     for (uint32_t i = threadIdx.x; i < CW; i += blockDim.x) ne_valid[i] = 0;
     if (threadIdx.x < 32) tile_cnt[threadIdx.x] = 0;
@@ -298,12 +303,12 @@ template <int AW>
 __global__ void __launch_bounds__(kAdmitWarps * 32) k_build_planes(
     uint32_t G, const uint32_t* __restrict__ goff, const uint8_t* __restrict__ lab, const uint64_t* __restrict__ sig_all,
     uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
-    int prof, uint32_t out_rows, uint64_t* __restrict__ out) {
+    int prof, uint32_t base, uint32_t out_rows, uint64_t* __restrict__ out) {
   extern __shared__ uint64_t tile[];  // [K * AW][32]
   const uint32_t GW = (G + 31u) / 32u;
   for (uint32_t gw = blockIdx.x; gw < GW; gw += gridDim.x) {
     __syncthreads();
-    fill_tile<AW, false>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, nullptr, 0, nullptr);
+    fill_tile<AW, false>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, base, nullptr, 0, nullptr);
     __syncthreads();
     uint4* dst = reinterpret_cast<uint4*>(out + static_cast<uint64_t>(gw) * out_rows * AW * 32);
     const uint4* src = reinterpret_cast<const uint4*>(tile);
@@ -394,7 +399,8 @@ int admit_launch(Queue* q, const Graph* query, const Graph* data, const uint64_t
   const uint64_t grid = std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms);
   k_planes_admit<AW, GATHER><<<grid, block, smem, q->stream>>>(
       G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, pp.K, pp.nlab, pp.spec, pp.r_begin,
-      q->opts.profile, rplanes, rrows, row_map, QG, query->graph_offsets, pp.C, pp.prog_off, pp.prog, pp.qc_off, pp.qc, n_qc,
+      q->opts.profile, data->vertex_base, rplanes, rrows, row_map, QG, query->graph_offsets, pp.C, pp.prog_off, pp.prog,
+      pp.qc_off, pp.qc, n_qc,
       n_prog, stage, planes, admit, counts);
   return check_launch(q, "k_planes_admit");
 }
@@ -494,7 +500,7 @@ int build_resident_planes(Queue* q, Graph* data, const uint64_t* sig_all, uint32
     k_build_planes<AWV><<<std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms), block, smem,      \
                           q->stream>>>(G, data->graph_offsets, data->node_labels, sig_all, N, R, K, nlab,            \
                                        static_cast<const uint32_t*>(dspec), static_cast<const uint32_t*>(drb),        \
-                                       q->opts.profile, out->rows, out->planes)
+                                       q->opts.profile, data->vertex_base, out->rows, out->planes)
     switch (AW) {
       case 1: SIGMO_BUILD(1); break;
       case 2: SIGMO_BUILD(2); break;

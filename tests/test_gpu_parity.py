@@ -329,3 +329,35 @@ def test_cli_driver_matches_oracle(tmp_path, extra):
         qb, db = oracle.parse_text(q.to_text()), oracle.parse_text(d.to_text())
         want = oracle.run_pipeline(qb, db, 3, oracle.REF_PTX, not find_all)["total"]
         assert got == want, (find_all, extra, got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ff", [False, True])
+def test_shards_keep_the_unsharded_results(ff):
+    """Data graphs split into contiguous shards (global vertex ids kept as a
+    vertex base): the shards' GMCR segments and per-pair counts, concatenated,
+    are the unsharded run's.  REF_PTX, where results depend on global ids."""
+    d = sb.generate_molecules(6000, 10, 60, seed=4801)
+    q = sb.generate_queries(60, 3, 20, seed=4802, skew_lo=5, skew_hi=12)
+    queue = sb.Queue(0)
+    qg, dg = sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)
+    gm = sb.GMCR(queue)
+    full = sb.match_batched(queue, qg, dg, 5, ff, None, gm)
+    off, idx = gm.getGMCR()
+    counts = gm.getPairCounts()
+    plan = sb.shard_plan(d, 3)
+    assert plan[1][2] >= 256 and sum(c for _, c, _ in plan) == d.num_graphs
+    tot, seg_idx, seg_cnt = 0, [], []
+    for first, count, base in plan:
+        sg = sb.createDeviceShard(queue, d, first, count)
+        gms = sb.GMCR(queue)
+        r = sb.match_batched(queue, qg, sg, 5, ff, None, gms)
+        o, i = gms.getGMCR()
+        assert np.array_equal(o.astype(np.int64), off[first:first + count + 1].astype(np.int64) - int(off[first]))
+        tot += r["total_matches"]
+        seg_idx.append(i)
+        seg_cnt.append(gms.getPairCounts())
+    assert tot == full["total_matches"]
+    assert np.array_equal(np.concatenate(seg_idx), idx) and np.array_equal(np.concatenate(seg_cnt), counts)
+    with pytest.raises(sb.SigmoError):
+        sb.createDeviceCSRGraph(queue, d.slice(10, 5)).set_vertex_base(100)

@@ -59,3 +59,39 @@ def test_two_gloo_ranks_run_independent_replicas():
     assert got[0][2] == got[1][2] == 11.0  # max over ranks
     assert got[0][3] == got[1][3] == float(want[0][0] + want[1][0])
     assert np.isfinite(got[0][3])
+
+
+def _shard_main(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    import torch
+
+    import oracle
+    import sigmo_b200 as sb
+
+    dist = bench.init_dist(world, "gloo")
+    q, d = bench.make_workload(WL, 0)
+    full = oracle.run_pipeline(q, d, WL["R"], oracle.REF_PTX, False)  # stands in for the shard's device run
+    first, count, base = sb.shard_plan(d, world)[rank]
+    off = full["offsets"].astype(np.int64)
+    mine = full["per_pair"][off[first]:off[first + count]].astype(np.int64)
+    # the exchange step: a sum of the counts and a gather of the per-pair lists
+    tot = torch.tensor([int(mine.sum())], dtype=torch.int64)
+    dist.all_reduce(tot)
+    parts = [None] * world
+    dist.all_gather_object(parts, mine.tolist())
+    out[rank] = (int(tot.item()), [x for p in parts for x in p], int(full["total"]), full["per_pair"].astype(np.int64).tolist())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_two_gloo_ranks_merge_shards_into_the_unsharded_result():
+    world = 2
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_shard_main, args=(world, _free_port(), out), nprocs=world, join=True)
+        got = dict(out)
+    for r in range(world):
+        tot, merged, want_tot, want_per = got[r]
+        assert tot == want_tot and merged == want_per
