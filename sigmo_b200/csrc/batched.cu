@@ -14,7 +14,21 @@
 namespace sigmo_b200 {
 namespace {
 
+void free_groups(Queue* q, PlaneProgram* pp) {
+  for (PlaneGroup& g : pp->groups) {
+    dev_free(q, g.spec);
+    dev_free(q, g.r_begin);
+    dev_free(q, g.row_of);
+    dev_free(q, g.prog_off);
+    dev_free(q, g.prog);
+    dev_free(q, g.qc_off);
+    dev_free(q, g.qc);
+  }
+  pp->groups.clear();
+}
+
 void free_program(Queue* q, PlaneProgram* pp) {
+  free_groups(q, pp);
   dev_free(q, pp->spec);
   dev_free(q, pp->prog_off);
   dev_free(q, pp->prog);
@@ -152,6 +166,130 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   return SIGMO_OK;
 }
 
+// Splits the query graphs into contiguous groups whose planes and classes fit
+// one admission tile (kGroupSmemBudget), greedily in query order, and uploads
+// each group's program in local plane / class ids.  off/list: every query
+// graph's classes in evaluation order (global class ids).
+int plan_groups(Queue* q, Graph* query, uint32_t AW, const std::vector<uint32_t>& off, const std::vector<uint32_t>& list) {
+  PlaneProgram& pp = query->pp;
+  const uint32_t QG = query->num_graphs, K = pp.K, C = pp.C, R = pp.R;
+  std::vector<uint32_t> plane_mark(K, 0), class_mark(C, 0);  // stamp = group number + 1
+  uint32_t stamp = 0, Kg = 0, Cg = 0, q0 = 0;
+  std::vector<std::pair<uint32_t, uint32_t>> ranges;
+  auto query_adds = [&](uint32_t qg, uint32_t* dk, uint32_t* dc) {
+    *dk = *dc = 0;
+    std::vector<uint32_t> seen_planes;
+    for (uint32_t e = off[qg]; e < off[qg + 1]; ++e) {
+      const uint32_t c = list[e];
+      if (class_mark[c] == stamp) continue;
+      ++*dc;
+      for (uint32_t i = pp.h_prog_off[c]; i < pp.h_prog_off[c + 1]; ++i) {
+        const uint32_t k = pp.h_prog[i];
+        if (plane_mark[k] != stamp && std::find(seen_planes.begin(), seen_planes.end(), k) == seen_planes.end()) {
+          seen_planes.push_back(k);
+          ++*dk;
+        }
+      }
+    }
+  };
+  auto take = [&](uint32_t qg) {
+    for (uint32_t e = off[qg]; e < off[qg + 1]; ++e) {
+      const uint32_t c = list[e];
+      if (class_mark[c] == stamp) continue;
+      class_mark[c] = stamp;
+      ++Cg;
+      for (uint32_t i = pp.h_prog_off[c]; i < pp.h_prog_off[c + 1]; ++i)
+        if (plane_mark[pp.h_prog[i]] != stamp) {
+          plane_mark[pp.h_prog[i]] = stamp;
+          ++Kg;
+        }
+    }
+  };
+  stamp = 1;
+  for (uint32_t qg = 0; qg < QG; ++qg) {
+    uint32_t dk, dc;
+    query_adds(qg, &dk, &dc);
+    if (qg > q0 && planes_admit_smem(Kg + dk, AW, Cg + dc) > kGroupSmemBudget) {
+      ranges.emplace_back(q0, qg);
+      ++stamp;
+      Kg = Cg = 0;
+      q0 = qg;
+    }
+    take(qg);
+    if (planes_admit_smem(Kg, AW, Cg) > 200u * 1024u)
+      return fail(SIGMO_ERR_DOMAIN, "query graph %u alone needs more than one admission tile of shared memory", qg);
+  }
+  ranges.emplace_back(q0, QG);
+  // each group's arrays, in local ids (planes in global order, so label
+  // planes come first and thresholds stay grouped by iteration)
+  for (size_t gi = 0; gi < ranges.size(); ++gi) {
+    PlaneGroup grp;
+    grp.q0 = ranges[gi].first;
+    grp.q1 = ranges[gi].second;
+    // this group's planes: those of its own queries' classes (marks from the
+    // planning pass may have been overwritten by a later group sharing a plane)
+    std::vector<uint8_t> in_group(K, 0);
+    for (uint32_t qg = grp.q0; qg < grp.q1; ++qg)
+      for (uint32_t e = off[qg]; e < off[qg + 1]; ++e)
+        for (uint32_t i = pp.h_prog_off[list[e]]; i < pp.h_prog_off[list[e] + 1]; ++i) in_group[pp.h_prog[i]] = 1;
+    std::vector<uint32_t> loc_plane(K, 0xFFFFFFFFu), spec, row_of, r_begin(R + 1, 0xFFFFFFFFu);
+    for (uint32_t k = 0; k < K; ++k)
+      if (in_group[k]) {
+        loc_plane[k] = static_cast<uint32_t>(spec.size());
+        spec.push_back(pp.h_spec[k]);
+        row_of.push_back(k);
+      }
+    uint32_t nlab = 0;
+    for (uint32_t i = 0; i < spec.size(); ++i) {
+      if (spec[i] & 0x80000000u) {
+        ++nlab;
+      } else {
+        const uint32_t r = (spec[i] >> 16) & 0xFFu;
+        r_begin[r] = std::min(r_begin[r], i);
+      }
+    }
+    r_begin[R] = static_cast<uint32_t>(spec.size());
+    for (int r = static_cast<int>(R) - 1; r >= 0; --r) r_begin[r] = std::min(r_begin[r], r_begin[r + 1]);
+    std::vector<uint32_t> loc_class(C, 0xFFFFFFFFu), prog_off{0}, qc_off{0}, qc;
+    std::vector<uint16_t> prog;
+    for (uint32_t qg = grp.q0; qg < grp.q1; ++qg) {
+      for (uint32_t e = off[qg]; e < off[qg + 1]; ++e) {
+        const uint32_t c = list[e];
+        if (loc_class[c] == 0xFFFFFFFFu) {
+          loc_class[c] = static_cast<uint32_t>(prog_off.size() - 1);
+          for (uint32_t i = pp.h_prog_off[c]; i < pp.h_prog_off[c + 1]; ++i)
+            prog.push_back(static_cast<uint16_t>(loc_plane[pp.h_prog[i]]));
+          prog_off.push_back(static_cast<uint32_t>(prog.size()));
+        }
+        qc.push_back(loc_class[c]);
+      }
+      qc_off.push_back(static_cast<uint32_t>(qc.size()));
+    }
+    grp.K = static_cast<uint32_t>(spec.size());
+    grp.C = static_cast<uint32_t>(prog_off.size() - 1);
+    // every local id the kernel will index with must be inside its array
+    for (uint16_t k : prog)
+      if (k >= grp.K) return fail(SIGMO_ERR_INVALID, "internal: group %zu plane %u outside its %u planes", gi, k, grp.K);
+    for (uint32_t c : qc)
+      if (c >= grp.C) return fail(SIGMO_ERR_INVALID, "internal: group %zu class %u outside its %u classes", gi, c, grp.C);
+    if (planes_admit_smem(grp.K, AW, grp.C) > 200u * 1024u)
+      return fail(SIGMO_ERR_DOMAIN, "group %zu needs more than one admission tile of shared memory", gi);
+    grp.nlab = nlab;
+    grp.n_qc = qc.size();
+    grp.n_prog = prog.size();
+    SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.spec), spec.data(), 4 * spec.size()));
+    SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.r_begin), r_begin.data(), 4 * r_begin.size()));
+    SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.row_of), row_of.data(), 4 * row_of.size()));
+    SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.prog_off), prog_off.data(), 4 * prog_off.size()));
+    SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.prog), prog.data(), 2 * prog.size()));
+    SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.qc_off), qc_off.data(), 4 * qc_off.size()));
+    SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.qc), qc.data(), 4 * qc.size()));
+    SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
+    pp.groups.push_back(grp);
+  }
+  return SIGMO_OK;
+}
+
 // Per query graph, its distinct classes in the order the admission kernel
 // evaluates them for `data`: rarest label first (the data graphs' vertex
 // counts per label), then longer programs (more thresholds) first, so a
@@ -182,10 +320,13 @@ int order_classes(Queue* q, Graph* query, Graph* data) {
   pp.qc_off = pp.qc = nullptr;
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.qc_off), off.data(), 4 * off.size()));
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.qc), list.data(), 4 * list.size()));
+  pp.h_qc_n = list.size();
+  free_groups(q, &pp);
+  const uint32_t AW = data->adj_words;
+  if (planes_admit_smem(pp.K, AW, pp.C) > kGroupSmemBudget) SIGMO_TRY(plan_groups(q, query, AW, off, list));
   SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
   pp.qc_for = data;
   pp.qc_stamp = data->stamp;
-  pp.h_qc_n = list.size();
   return SIGMO_OK;
 }
 
@@ -314,9 +455,15 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   }
   if (!rc) rc = mark(1);
   if (!rc) rc = order_classes(q, query, data);
-  if (!rc)
+  if (!rc && !rp && !pp.groups.empty()) {
+    // a batch too large for one tile: group by group into the batch's planes
+    if (cudaMemsetAsync(adm_counts, 0, 4ull * G, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
+    for (size_t gi = 0; gi < pp.groups.size() && !rc; ++gi)
+      rc = launch_planes_admit_group(q, query, data, dsig, R, pp.groups[gi], pp.K, planes, admit, adm_counts);
+  } else if (!rc) {
     rc = rp ? launch_planes_admit_resident(q, query, data, *rp, pp, d_row_map, admit, adm_counts)
             : launch_planes_admit(q, query, data, dsig, R, pp, planes, admit, adm_counts);
+  }
   if (!rc) rc = mark(2);
   // captured: the admitted total of the run that built the graph sizes the
   // arrays (the replay checks that it did not change)
@@ -464,7 +611,14 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   uint64_t* d_total = nullptr;
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
   int rc = cudaMemsetAsync(d_total, 0, 8, q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "memset failed");
-  const bool planes_fit = planes_admit_smem(query->pp.K, data->adj_words, query->pp.C) <= 200u * 1024u;
+  // the planes route takes any batch whose query graphs each fit an admission
+  // tile (larger batches are admitted in groups); planes take 8 B per
+  // (plane, graph, word) in device memory
+  int prc = order_classes(q, query, data);
+  if (prc == SIGMO_ERR_DOMAIN) prc = SIGMO_OK;  // a query graph too large for a tile: bitset route
+  else if (prc) return prc;
+  const bool planes_fit = query->pp.qc_for == data && (!query->pp.groups.empty() ||
+                                                       planes_admit_smem(query->pp.K, data->adj_words, query->pp.C) <= 200u * 1024u);
   const bool bitset_route = materialize || !planes_fit;
   if (!rc && bitset_route && data->vertex_base)
     rc = fail(SIGMO_ERR_DOMAIN, "a shard (vertex base %u) runs on the planes route only; this batch needs the bitset route",

@@ -44,6 +44,23 @@ struct Queue {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
+// A contiguous range of query graphs whose planes and classes fit one
+// k_planes_admit tile in shared memory (a batch too large for one tile is
+// admitted group by group).  Device arrays are in group-local plane and class
+// ids; row_of maps a local plane to its row in the batch's plane array.
+struct PlaneGroup {
+  uint32_t q0 = 0, q1 = 0;
+  uint32_t K = 0, C = 0, nlab = 0;
+  uint32_t* spec = nullptr;      // [K]
+  uint32_t* r_begin = nullptr;   // [R + 1]
+  uint32_t* row_of = nullptr;    // [K] plane row in the batch
+  uint32_t* prog_off = nullptr;  // [C + 1]
+  uint16_t* prog = nullptr;      // local plane ids
+  uint32_t* qc_off = nullptr;    // [q1 - q0 + 1]
+  uint32_t* qc = nullptr;        // local class ids in evaluation order
+  size_t n_qc = 0, n_prog = 0;
+};
+
 // Per-query-batch plane program of the batched form (kernels_planes.cu).
 struct PlaneProgram {
   bool valid = false;
@@ -66,6 +83,7 @@ struct PlaneProgram {
   uint32_t* qc_off = nullptr;     // [query graphs + 1]
   uint32_t* qc = nullptr;
   size_t h_qc_n = 0;              // entries of qc
+  std::vector<PlaneGroup> groups; // empty: the whole batch fits one tile
   const void* qc_for = nullptr;   // the data graph the order was built for
   uint64_t qc_stamp = 0;
   uint64_t* qsig_all = nullptr;   // [R][query vertices] signatures, iterations 1..R
@@ -193,6 +211,13 @@ int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const u
                         bool sync_total, uint64_t capacity_hint);
 int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
                         const PlaneProgram& pp, uint64_t* planes, uint32_t* admit, uint32_t* counts);
+// One group of a batch: its planes go to their rows of the batch's planes
+// (K_total rows per tile), its admission words to its query graphs' rows, and
+// its per-graph admitted counts are added to counts.
+int launch_planes_admit_group(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
+                              const PlaneGroup& grp, uint32_t K_total, uint64_t* planes, uint32_t* admit, uint32_t* counts);
+// Shared memory of one k_planes_admit tile for K planes and C classes.
+constexpr size_t kGroupSmemBudget = 96u * 1024u;
 // The same admission with the tile's planes gathered from resident planes
 // (row_map[k] = resident row of the batch's plane k).
 int launch_planes_admit_resident(Queue* q, const Graph* query, const Graph* data, const ResidentPlanes& rp,

@@ -194,7 +194,8 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     uint32_t QG,
     const uint32_t* __restrict__ qgoff, uint32_t C, const uint32_t* __restrict__ g_prog_off, const uint16_t* __restrict__ g_prog,
     const uint32_t* __restrict__ g_qc_off, const uint32_t* __restrict__ g_qc, uint32_t n_qc, uint32_t n_prog, int stage_lists,
-    uint64_t* __restrict__ planes, uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
+    const uint32_t* __restrict__ row_of, uint32_t out_rows, int accumulate, uint64_t* __restrict__ planes,
+    uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t tile_cnt[32];
   constexpr uint32_t kRow = AW * 32u;
@@ -244,9 +245,19 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     if (threadIdx.x < 32) tile_cnt[threadIdx.x] = 0;
     __syncthreads();
     if (!GATHER) {
-      uint4* dst = reinterpret_cast<uint4*>(planes + static_cast<uint64_t>(gw) * words * 32);
-      const uint4* src = reinterpret_cast<const uint4*>(tile);
-      for (uint32_t i = threadIdx.x; i < words * 16; i += blockDim.x) dst[i] = src[i];
+      if (!row_of) {  // the batch's planes: this tile's rows, contiguous
+        uint4* dst = reinterpret_cast<uint4*>(planes + static_cast<uint64_t>(gw) * words * 32);
+        const uint4* src = reinterpret_cast<const uint4*>(tile);
+        for (uint32_t i = threadIdx.x; i < words * 16; i += blockDim.x) dst[i] = src[i];
+      } else {  // one group of the batch: local row k goes to row row_of[k] of out_rows
+        constexpr uint32_t kChunks = AW * 16u;  // 16-byte chunks per row
+        uint64_t* dst = planes + static_cast<uint64_t>(gw) * out_rows * kRow;
+        for (uint32_t i = threadIdx.x; i < K * kChunks; i += blockDim.x) {
+          const uint32_t k = i / kChunks, c = i % kChunks;
+          reinterpret_cast<uint4*>(dst + static_cast<uint64_t>(row_of[k]) * kRow)[c] =
+              reinterpret_cast<const uint4*>(tile + k * kRow)[c];
+        }
+      }
     }
     const uint64_t* tl = tile + lane;
     const uint32_t in_tile = G - gw * 32u;
@@ -291,7 +302,10 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     }
     atomicAdd(&tile_cnt[lane], my_cnt);
     __syncthreads();
-    if (threadIdx.x < 32 && gw * 32u + threadIdx.x < G) counts[gw * 32u + threadIdx.x] = tile_cnt[threadIdx.x];
+    if (threadIdx.x < 32 && gw * 32u + threadIdx.x < G) {
+      if (accumulate) atomicAdd(&counts[gw * 32u + threadIdx.x], tile_cnt[threadIdx.x]);
+      else counts[gw * 32u + threadIdx.x] = tile_cnt[threadIdx.x];
+    }
     buf ^= GATHER ? 1u : 0u;
   }
   if (GATHER) cp_async_wait_all();
@@ -378,17 +392,27 @@ size_t planes_admit_smem(uint32_t K, uint32_t AW, uint32_t C) {
 
 namespace {
 
+// What one admission launch needs of a program: the whole batch's, or one
+// group's (local ids; planes scattered to row_of).
+struct AdmitView {
+  uint32_t K, C, nlab, QG;
+  const uint32_t *spec, *r_begin, *prog_off, *qc_off, *qc, *qgoff, *row_of;
+  const uint16_t* prog;
+  size_t n_qc, n_prog;
+  uint32_t out_rows;
+  int accumulate;
+};
+
 template <int AW, bool GATHER>
-int admit_launch(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R, const PlaneProgram& pp,
-                 const uint64_t* rplanes, uint32_t rrows, const uint32_t* row_map, uint64_t* planes, uint32_t* admit,
-                 uint32_t* counts) {
-  const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, QG = query->num_graphs;
-  const uint32_t n_qc = static_cast<uint32_t>(pp.h_qc_n), n_prog = static_cast<uint32_t>(pp.h_prog.size());
-  const size_t list_bytes = 4ull * (QG + 1 + n_qc + pp.C + 1) + 2ull * n_prog;
-  const size_t base = admit_smem_layout(pp.K, AW, pp.C, GATHER, 0).total;
+int admit_launch(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t R, const AdmitView& v, const uint64_t* rplanes,
+                 uint32_t rrows, const uint32_t* row_map, uint64_t* planes, uint32_t* admit, uint32_t* counts) {
+  const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, QG = v.QG;
+  const uint32_t n_qc = static_cast<uint32_t>(v.n_qc), n_prog = static_cast<uint32_t>(v.n_prog);
+  const size_t list_bytes = 4ull * (QG + 1 + n_qc + v.C + 1) + 2ull * n_prog;
+  const size_t base = admit_smem_layout(v.K, AW, v.C, GATHER, 0).total;
   // stage the class lists when the block still fits three to an SM
   const int stage = base + list_bytes <= 72u * 1024u ? 1 : 0;
-  const size_t smem = admit_smem_layout(pp.K, AW, pp.C, GATHER, stage ? list_bytes : 0).total;
+  const size_t smem = admit_smem_layout(v.K, AW, v.C, GATHER, stage ? list_bytes : 0).total;
   if (smem > 220u * 1024u) return fail(SIGMO_ERR_DOMAIN, "k_planes_admit needs %zu bytes of shared memory", smem);
   const unsigned block = 32u * kAdmitWarps;
   int per_sm = 0, sms = 0;
@@ -398,11 +422,16 @@ int admit_launch(Queue* q, const Graph* query, const Graph* data, const uint64_t
   if (e != cudaSuccess) return fail(SIGMO_ERR_CUDA, "k_planes_admit shared-memory setup failed: %s", cudaGetErrorString(e));
   const uint64_t grid = std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms);
   k_planes_admit<AW, GATHER><<<grid, block, smem, q->stream>>>(
-      G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, pp.K, pp.nlab, pp.spec, pp.r_begin,
-      q->opts.profile, data->vertex_base, rplanes, rrows, row_map, QG, query->graph_offsets, pp.C, pp.prog_off, pp.prog,
-      pp.qc_off, pp.qc, n_qc,
-      n_prog, stage, planes, admit, counts);
+      G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, v.K, v.nlab, v.spec, v.r_begin, q->opts.profile,
+      data->vertex_base, rplanes, rrows, row_map, QG, v.qgoff, v.C, v.prog_off, v.prog, v.qc_off, v.qc, n_qc, n_prog, stage,
+      v.row_of, v.out_rows, v.accumulate, planes, admit, counts);
   return check_launch(q, "k_planes_admit");
+}
+
+AdmitView whole_batch(const Graph* query, const PlaneProgram& pp) {
+  return AdmitView{pp.K,      pp.C,       pp.nlab,  query->num_graphs, pp.spec, pp.r_begin, pp.prog_off,
+                   pp.qc_off, pp.qc,      query->graph_offsets, nullptr, pp.prog, pp.h_qc_n, pp.h_prog.size(),
+                   pp.K,      0};
 }
 
 }  // namespace
@@ -410,20 +439,37 @@ int admit_launch(Queue* q, const Graph* query, const Graph* data, const uint64_t
 int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
                         const PlaneProgram& pp, uint64_t* planes, uint32_t* admit, uint32_t* counts) {
   if (!data->num_graphs) return SIGMO_OK;
+  const AdmitView v = whole_batch(query, pp);
   switch (data->adj_words) {
-    case 1: return admit_launch<1, false>(q, query, data, sig_all, R, pp, nullptr, 0, nullptr, planes, admit, counts);
-    case 2: return admit_launch<2, false>(q, query, data, sig_all, R, pp, nullptr, 0, nullptr, planes, admit, counts);
-    default: return admit_launch<4, false>(q, query, data, sig_all, R, pp, nullptr, 0, nullptr, planes, admit, counts);
+    case 1: return admit_launch<1, false>(q, data, sig_all, R, v, nullptr, 0, nullptr, planes, admit, counts);
+    case 2: return admit_launch<2, false>(q, data, sig_all, R, v, nullptr, 0, nullptr, planes, admit, counts);
+    default: return admit_launch<4, false>(q, data, sig_all, R, v, nullptr, 0, nullptr, planes, admit, counts);
+  }
+}
+
+int launch_planes_admit_group(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
+                              const PlaneGroup& grp, uint32_t K_total, uint64_t* planes, uint32_t* admit, uint32_t* counts) {
+  if (!data->num_graphs || grp.q1 <= grp.q0) return SIGMO_OK;
+  const uint32_t GW = (data->num_graphs + 31u) / 32u;
+  const AdmitView v{grp.K,      grp.C,  grp.nlab, grp.q1 - grp.q0, grp.spec, grp.r_begin, grp.prog_off,
+                    grp.qc_off, grp.qc, query->graph_offsets + grp.q0, grp.row_of, grp.prog, grp.n_qc, grp.n_prog,
+                    K_total,    1};
+  uint32_t* adm = admit + static_cast<uint64_t>(grp.q0) * GW;
+  switch (data->adj_words) {
+    case 1: return admit_launch<1, false>(q, data, sig_all, R, v, nullptr, 0, nullptr, planes, adm, counts);
+    case 2: return admit_launch<2, false>(q, data, sig_all, R, v, nullptr, 0, nullptr, planes, adm, counts);
+    default: return admit_launch<4, false>(q, data, sig_all, R, v, nullptr, 0, nullptr, planes, adm, counts);
   }
 }
 
 int launch_planes_admit_resident(Queue* q, const Graph* query, const Graph* data, const ResidentPlanes& rp,
                                  const PlaneProgram& pp, const uint32_t* row_map, uint32_t* admit, uint32_t* counts) {
   if (!data->num_graphs) return SIGMO_OK;
+  const AdmitView v = whole_batch(query, pp);
   switch (data->adj_words) {
-    case 1: return admit_launch<1, true>(q, query, data, nullptr, 0, pp, rp.planes, rp.rows, row_map, nullptr, admit, counts);
-    case 2: return admit_launch<2, true>(q, query, data, nullptr, 0, pp, rp.planes, rp.rows, row_map, nullptr, admit, counts);
-    default: return admit_launch<4, true>(q, query, data, nullptr, 0, pp, rp.planes, rp.rows, row_map, nullptr, admit, counts);
+    case 1: return admit_launch<1, true>(q, data, nullptr, 0, v, rp.planes, rp.rows, row_map, nullptr, admit, counts);
+    case 2: return admit_launch<2, true>(q, data, nullptr, 0, v, rp.planes, rp.rows, row_map, nullptr, admit, counts);
+    default: return admit_launch<4, true>(q, data, nullptr, 0, v, rp.planes, rp.rows, row_map, nullptr, admit, counts);
   }
 }
 

@@ -361,3 +361,17 @@ def test_shards_keep_the_unsharded_results(ff):
     assert np.array_equal(np.concatenate(seg_idx), idx) and np.array_equal(np.concatenate(seg_cnt), counts)
     with pytest.raises(sb.SigmoError):
         sb.createDeviceCSRGraph(queue, d.slice(10, 5)).set_vertex_base(100)
+
+
+@pytest.mark.gpu
+def test_query_batch_admitted_in_groups():
+    """A query batch whose planes and classes exceed one admission tile
+    (1,000 queries of 3-40 atoms: ~17k classes; molecules up to 120 atoms,
+    two words per vertex set) is admitted group by group into one plane
+    array; GMCR and per-pair counts equal the oracle's."""
+    d = sb.generate_molecules(1500, 6, 120, seed=4903, kind=1, median=22.0)
+    q = sb.generate_queries(1000, 3, 40, seed=4901)
+    assert d.sizes().max() > 64
+    ref = _oracle(q, d, 4, oracle.REF_PTX, False)
+    got = run_both_batched(q, d, 4, oracle.REF_PTX, False)
+    _check(got, ref, "grouped admission")
