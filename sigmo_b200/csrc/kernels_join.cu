@@ -647,7 +647,8 @@ constexpr uint32_t kPhaseLevels = 16;
 constexpr uint32_t kPhaseThreads = 256;
 
 __global__ void __launch_bounds__(256) k_pair_masks(
-    const uint64_t* __restrict__ planes, uint32_t K, const uint32_t* __restrict__ prog_off, const uint16_t* __restrict__ prog,
+    const uint64_t* __restrict__ planes, uint32_t K, uint32_t AW, const uint32_t* __restrict__ prog_off,
+    const uint16_t* __restrict__ prog,
     const uint32_t* __restrict__ cls, const uint32_t* __restrict__ qgoff, const uint8_t* __restrict__ qorder,
     const uint8_t* __restrict__ qsym, const uint32_t* __restrict__ dgoff, const uint8_t* __restrict__ dsym,
     const uint32_t* __restrict__ indices, const uint32_t* __restrict__ pair_graph, uint64_t slot0, uint64_t count,
@@ -663,24 +664,29 @@ __global__ void __launch_bounds__(256) k_pair_masks(
     if (j >= n) continue;
     const uint32_t g = pair_graph[slot];
     const bool ident = !(qsym[qg] && dsym[g]);
-    if (j == 0) {  // the pair's setup record: first data vertex, query size, query offset, order
-      rec[local] = make_uint4(dgoff[g], n | (ident ? 0x100u : 0u), qoff, g);
-      if (n > kPhaseLevels && g >= skip_below) {  // joined by the generic kernel, which accumulates into counts
+    // queries over kPhaseLevels vertices and molecules over 64 atoms (a
+    // vertex set wider than one word) go to the generic kernel
+    const bool generic = n > kPhaseLevels || dgoff[g + 1] - dgoff[g] > 64u;
+    if (j == 0) {  // the pair's setup record: first data vertex, query size | flags, query offset, data graph
+      rec[local] = make_uint4(dgoff[g], n | (ident ? 0x100u : 0u) | (generic ? 0x200u : 0u), qoff, g);
+      if (generic && g >= skip_below) {  // joined by the generic kernel, which accumulates into counts
         overflow[atomicAdd(overflow_len, 1ull)] = static_cast<uint32_t>(slot);
         counts[slot] = 0;
       }
     }
-    if (n > kPhaseLevels) continue;
+    if (generic) continue;
     const uint32_t c = cls[qoff + (ident ? j : qorder[qoff + j])];
-    const uint64_t* base = planes + static_cast<uint64_t>(g >> 5) * K * 32 + (g & 31u);
+    // word 0 of each plane: the graph's vertex set fits one word
+    const uint64_t* base = planes + static_cast<uint64_t>(g >> 5) * K * AW * 32 + (g & 31u);
     uint64_t m = ~0ull;
     const uint32_t e1 = prog_off[c + 1];
-    for (uint32_t e = prog_off[c]; e < e1; ++e) m &= base[static_cast<uint64_t>(prog[e]) * 32];
+    for (uint32_t e = prog_off[c]; e < e1; ++e) m &= base[static_cast<uint64_t>(prog[e]) * AW * 32];
     masks[static_cast<uint64_t>(j) * count + local] = m;
   }
 }
 
-template <bool EXACT>
+// DAW: words per adjacency row of the data batch (the pairs here use word 0).
+template <bool EXACT, uint32_t DAW>
 __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
     const uint64_t* __restrict__ masks, const uint4* __restrict__ rec, uint64_t slot0, uint64_t count,
     const uint64_t* __restrict__ qsel, const uint64_t* __restrict__ qsel_id, const uint64_t* __restrict__ dadj,
@@ -722,7 +728,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
       const uint4 r = rec[local];  // first data vertex, query size | order flag, query offset, data graph
       if (r.w < skip_below) continue;
       n = r.y & 0xFFu;
-      if (n > kPhaseLevels) continue;  // in the overflow list (generic kernel)
+      if (r.y & 0x200u) continue;  // in the overflow list (generic kernel)
       s = r.x;
       selp = ((r.y & 0x100u) ? qsel_id : qsel) + r.z;
       AT(cand, 0) = masks[local];
@@ -741,7 +747,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
     }
     const uint32_t t = __ffsll(static_cast<long long>(ck)) - 1;
     AT(cand, k) = ck & (ck - 1);
-    const uint64_t rw = dadj[s + t];
+    const uint64_t rw = dadj[static_cast<uint64_t>(s + t) * DAW];
     const uint64_t keep = 0ull - ((selp[k + 1] >> k) & 1ull);
     uint64_t nx = AT(base, k + 1) & ~(rw ^ keep);
     if (EXACT) nx &= ~(used | (1ull << t));
@@ -756,7 +762,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
     AT(cand, k + 1) = nx;
     const uint64_t sl2 = selp[k + 2];
     uint64_t b2 = masks[static_cast<uint64_t>(k + 2) * count + local] & ~(rw ^ (0ull - ((sl2 >> k) & 1ull)));
-    for (int i = 0; i < k; ++i) b2 &= ~(dadj[s + AT(pk, i)] ^ (0ull - ((sl2 >> i) & 1ull)));
+    for (int i = 0; i < k; ++i) b2 &= ~(dadj[static_cast<uint64_t>(s + AT(pk, i)) * DAW] ^ (0ull - ((sl2 >> i) & 1ull)));
     AT(base, k + 2) = b2;
     ++k;
   }
@@ -866,24 +872,31 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
   uint32_t* overflow = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + 256);
   SIGMO_CUDA_TRY(cudaMemsetAsync(ctr, 0, 256, q->stream));
   auto* tot = reinterpret_cast<unsigned long long*>(d_total);
-  // two-phase route for data graphs of <= 64 vertices, in chunks of slots
-  const bool tiles = data->adj_words == 1;
+  // two-phase join, in chunks of slots, for the pairs of queries of <= 16
+  // vertices and molecules of <= 64 atoms; the rest go to the overflow list
   int rc = SIGMO_OK;
-  if (tiles) {
+  {
     const sigmo_tuning& tn = q->tune;
     const uint64_t chunk = std::min<uint64_t>(m->total, static_cast<uint64_t>(tn.mask_chunk_slots) << 20);
     void* mbuf = nullptr;
     rc = dev_alloc(q, &mbuf, 8ull * kPhaseLevels * chunk + 16ull * chunk);
     const size_t smem = static_cast<size_t>(kPhaseLevels) * kPhaseThreads * (2 * 8 + 1);
-    if (!rc)
-      rc = exact ? allow_max_dynamic_smem(reinterpret_cast<const void*>(k_join_masks<true>), q->device)
-                 : allow_max_dynamic_smem(reinterpret_cast<const void*>(k_join_masks<false>), q->device);
+    // the kernel for this batch's adjacency-row width and profile
+    void (*join_kernel)(const uint64_t*, const uint4*, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const uint64_t*,
+                        uint32_t, int, uint32_t, unsigned long long*, uint64_t*, unsigned long long*) = nullptr;
+    switch (data->adj_words) {
+      case 1: join_kernel = exact ? k_join_masks<true, 1> : k_join_masks<false, 1>; break;
+      case 2: join_kernel = exact ? k_join_masks<true, 2> : k_join_masks<false, 2>; break;
+      default: join_kernel = exact ? k_join_masks<true, 4> : k_join_masks<false, 4>; break;
+    }
+    if (!rc) rc = allow_max_dynamic_smem(reinterpret_cast<const void*>(join_kernel), q->device);
     for (uint64_t slot0 = 0; slot0 < m->total && !rc; slot0 += chunk) {
       const uint64_t cnt = std::min<uint64_t>(chunk, m->total - slot0);
       auto* masks = static_cast<uint64_t*>(mbuf);
       auto* recs = reinterpret_cast<uint4*>(masks + kPhaseLevels * chunk);
       k_pair_masks<<<grid_for(cnt * kPhaseLevels, 256, 148u * 32u), 256, 0, q->stream>>>(
-          planes, planes_rows, pp.prog_off, prog, pp.cls, query->graph_offsets, query->qorder, query->sym, data->graph_offsets,
+          planes, planes_rows, data->adj_words, pp.prog_off, prog, pp.cls, query->graph_offsets, query->qorder, query->sym,
+          data->graph_offsets,
           data->sym, m->indices, m->pair_graph, slot0, cnt, masks, recs, skip, overflow, ctr + 2, m->counts);
       rc = check_launch(q, "k_pair_masks");
       if (!rc && slot0 + chunk >= m->total && cudaEventRecord(q->ev_fork, q->stream) != cudaSuccess)
@@ -893,21 +906,15 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device);
         const unsigned grid = static_cast<unsigned>(sms) * tn.join_blocks_per_sm;
-        if (exact)
-          k_join_masks<true><<<grid, kPhaseThreads, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id,
-                                                                         data->adj, skip, find_first, tn.join_chunk, ctr,
-                                                                         m->counts, tot);
-        else
-          k_join_masks<false><<<grid, kPhaseThreads, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id,
-                                                                          data->adj, skip, find_first, tn.join_chunk, ctr,
-                                                                          m->counts, tot);
+        join_kernel<<<grid, kPhaseThreads, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id, data->adj,
+                                                              skip, find_first, tn.join_chunk, ctr, m->counts, tot);
         rc = check_launch(q, "k_join_masks");
       }
     }
     dev_free(q, mbuf);
   }
   const cudaStream_t main_stream = q->stream;
-  const bool side = tiles && !q->tune.overflow_serial;
+  const bool side = !q->tune.overflow_serial;
   if (!rc && side) {
     // the overflow list is complete after the last Phase A: its pairs run on
     // the side stream, overlapping Phase B (the caller joins the side stream)
@@ -915,12 +922,12 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
     q->stream = q->side;
   }
   if (!rc) {
-    // the overflow list (two-phase route) or every slot (otherwise) through the generic kernel
+    // the overflow list through the generic kernel
     const unsigned block = 128;
-    const unsigned grid = tiles ? q->tune.overflow_blocks : 148u * 8u;
-    const uint32_t* list = tiles ? overflow : nullptr;
-    const uint32_t split = tiles ? q->tune.overflow_split : 1u;
-    const unsigned long long* list_len = tiles ? ctr + 2 : nullptr;
+    const unsigned grid = q->tune.overflow_blocks;
+    const uint32_t* list = overflow;
+    const uint32_t split = q->tune.overflow_split;
+    const unsigned long long* list_len = ctr + 2;
 #define SIGMO_JOIN_PLANES(AWV, EX)                                                                                      \
   k_join_fast<AWV, EX, true><<<grid, block, 0, q->stream>>>(nullptr, 0, planes, planes_rows, pp.prog_off, prog, pp.cls,  \
                                                             q->opts.profile, query->graph_offsets, query->qorder,        \
