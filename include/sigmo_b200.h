@@ -128,6 +128,8 @@ typedef struct sigmo_tuning {
   uint32_t mask_chunk_slots;     /* GMCR slots per level-mask pass, in 2^20 units, 1..64 (8)     */
   uint32_t overflow_split;       /* work items per pair of those queries, each taking every
                                     split-th root candidate, 1..64 (16)                          */
+  uint32_t join_kernel;          /* 0 (default): per-lane DFS machine; 1: warp-cooperative
+                                    frontier join (32 candidate tries per round, one per lane)   */
 } sigmo_tuning;
 /* sycl::queue{gpu_selector_v, enable_profiling} (library/src/sigmo.cpp:19). */
 SIGMO_API int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out);

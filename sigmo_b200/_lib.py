@@ -52,6 +52,7 @@ class TuningC(ctypes.Structure):
         ("overflow_serial", ctypes.c_uint32),
         ("mask_chunk_slots", ctypes.c_uint32),
         ("overflow_split", ctypes.c_uint32),
+        ("join_kernel", ctypes.c_uint32),
     ]
 
 

@@ -17,7 +17,7 @@
 namespace sigmo_b200 {
 
 int normalize_tuning(sigmo_tuning* t) {
-  const sigmo_tuning d{3, 4, 148 * 8, 1, 8, 16};
+  const sigmo_tuning d{3, 4, 148 * 8, 1, 8, 16, 0};
   if (!t->join_blocks_per_sm) t->join_blocks_per_sm = d.join_blocks_per_sm;
   if (!t->join_chunk) t->join_chunk = d.join_chunk;
   if (!t->overflow_blocks) t->overflow_blocks = d.overflow_blocks;
@@ -29,6 +29,7 @@ int normalize_tuning(sigmo_tuning* t) {
   if (t->overflow_serial > 1) return fail(SIGMO_ERR_INVALID, "overflow_serial must be 0 or 1");
   if (t->mask_chunk_slots > 64) return fail(SIGMO_ERR_INVALID, "mask_chunk_slots must be 1..64");
   if (t->overflow_split > 64) return fail(SIGMO_ERR_INVALID, "overflow_split must be 1..64");
+  if (t->join_kernel > 1) return fail(SIGMO_ERR_INVALID, "join_kernel must be 0 or 1");
   return SIGMO_OK;
 }
 

@@ -595,7 +595,8 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   const sigmo_tuning& tn = q->tune;
   const uint64_t key[6] = {query->stamp, data->stamp, R, static_cast<uint64_t>(find_first),
                            static_cast<uint64_t>(q->opts.profile) | (static_cast<uint64_t>(tn.overflow_serial) << 8) |
-                               (static_cast<uint64_t>(tn.overflow_split) << 16),
+                               (static_cast<uint64_t>(tn.overflow_split) << 16) |
+                               (static_cast<uint64_t>(tn.join_kernel) << 24),
                            (static_cast<uint64_t>(tn.join_blocks_per_sm) << 48) | (static_cast<uint64_t>(tn.join_chunk) << 40) |
                                (static_cast<uint64_t>(tn.mask_chunk_slots) << 32) | tn.overflow_blocks};
   if (graph && !materialize && m->graph && std::equal(key, key + 6, m->graph_key)) {
@@ -711,6 +712,7 @@ extern "C" int sigmo_autotune(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_
     std::vector<uint32_t> values;
   };
   const Axis axes[] = {
+      {&sigmo_tuning::join_kernel, {0, 1}},
       {&sigmo_tuning::overflow_serial, {0, 1}},
       {&sigmo_tuning::join_blocks_per_sm, {1, 2, 3}},
       {&sigmo_tuning::join_chunk, {1, 2, 4, 8, 16}},

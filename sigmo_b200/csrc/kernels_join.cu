@@ -771,6 +771,246 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
   if (lane == 0 && my_total) atomicAdd(d_total, static_cast<unsigned long long>(my_total));
 }
 
+// Position of the r-th (0-based) set bit of m; m has more than r set bits.
+__device__ __forceinline__ uint32_t nth_set32(uint32_t m, uint32_t r) {
+  uint32_t pos = 0, c = __popc(m & 0xFFFFu);
+  if (r >= c) { r -= c; pos += 16; m >>= 16; }
+  c = __popc(m & 0xFFu);
+  if (r >= c) { r -= c; pos += 8; m >>= 8; }
+  c = __popc(m & 0xFu);
+  if (r >= c) { r -= c; pos += 4; m >>= 4; }
+  c = __popc(m & 0x3u);
+  if (r >= c) { r -= c; pos += 2; m >>= 2; }
+  if (r >= (m & 1u)) pos += 1;
+  return pos;
+}
+__device__ __forceinline__ uint32_t nth_set64(uint64_t m, uint32_t r) {
+  const uint32_t lo = static_cast<uint32_t>(m), c = __popc(lo);
+  const bool up = r >= c;
+  return (up ? 32u : 0u) + nth_set32(up ? static_cast<uint32_t>(m >> 32) : lo, up ? r - c : r);
+}
+
+// Phase B, warp-cooperative form (k_join_frontier).  A warp keeps up to 32
+// pairs in flight (slot p: its root candidates, count and live-entry count).
+// A partial embedding of depth L >= 1 is an entry {candidates left at level
+// L; meta = pair | vertex placed at level L-1 << 5 | parent entry << 11} in a
+// per-warp pool where each level's entries form one region, stacked in level
+// order.  A round takes the next 32 (entry, candidate) items of the current
+// level L, one per lane: the lane rebuilds the level-(L+1) constraint by
+// walking the parent chain, tries its candidate (the same test as the
+// per-lane machine) and appends the child entry at level L+1, or adds the
+// popcount when L+1 is the last level.  The warp goes one level deeper once
+// the next level holds a full round (levels above kFrontDeep: any entry), and
+// back up when the current level is used up, so a level holds at most 63
+// entries (31 above kFrontDeep) and the pool is bounded by kFrontPool.
+// Counts are order-independent sums, so they equal the per-lane machine's.
+constexpr uint32_t kFrontPairs = 32;
+constexpr uint32_t kFrontDeep = 4;
+constexpr uint32_t kFrontPool = kFrontDeep * 63u + (kPhaseLevels - 2u - kFrontDeep) * 32u;
+constexpr uint32_t kFrontWarps = 8;
+constexpr uint32_t kFrontFree = 0xFFFFFFFFu;
+struct FrontWarp {
+  unsigned long long pcnt[kFrontPairs];  // embeddings found per pair slot
+  uint64_t pcand[kFrontPairs];           // level-0 candidates not yet taken
+  uint64_t ecand[kFrontPool];
+  uint32_t emeta[kFrontPool];
+  // per pair slot: first data vertex of the graph, query offset | identity-order
+  // flag << 31, chunk-local slot (kFrontFree when the slot is free), query size
+  uint4 pinfo[kFrontPairs];
+  uint32_t pref[kFrontPairs];  // live entries (root included)
+  uint16_t head[kPhaseLevels + 1], tail[kPhaseLevels + 1];
+};
+
+template <bool EXACT, uint32_t DAW>
+__global__ void __launch_bounds__(kFrontWarps * 32, 3) k_join_frontier(
+    const uint64_t* __restrict__ masks, const uint4* __restrict__ rec, uint64_t slot0, uint64_t count,
+    const uint64_t* __restrict__ qsel, const uint64_t* __restrict__ qsel_id, const uint64_t* __restrict__ dadj,
+    uint32_t skip_below, int find_first, uint32_t kChunk, unsigned long long* __restrict__ cursor,
+    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total) {
+  extern __shared__ __align__(16) unsigned char front_raw[];
+  FrontWarp& w = reinterpret_cast<FrontWarp*>(front_raw)[threadIdx.x >> 5];
+  const unsigned lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+  constexpr unsigned kAll = 0xFFFFFFFFu;
+  w.pinfo[lane].z = kFrontFree;
+  w.pcand[lane] = 0;
+  w.pref[lane] = 0;
+  if (lane <= kPhaseLevels) w.head[lane] = w.tail[lane] = 0;
+  __syncwarp();
+  uint64_t next = 0, end = 0;  // warp-uniform range of chunk-local slots
+  bool more = true;
+  uint64_t my_total = 0;
+  uint32_t L = 0;
+  for (;;) {
+    if (L == 0 && more) {
+      // fill the free pair slots (lane i owns slot i) from the work range
+      bool fr = w.pinfo[lane].z == kFrontFree;
+      unsigned F = __ballot_sync(kAll, fr);
+      while (F && more) {
+        if (next >= end) {
+          unsigned long long b = 0;
+          if (lane == 0) b = atomicAdd(cursor, 32ull * kChunk);
+          b = __shfl_sync(kAll, b, 0);
+          next = b;
+          end = b + 32ull * kChunk < count ? b + 32ull * kChunk : count;
+          if (next >= count) {
+            more = false;
+            break;
+          }
+        }
+        const uint32_t avail = static_cast<uint32_t>(end - next < 32 ? end - next : 32);
+        const uint32_t take = min(static_cast<uint32_t>(__popc(F)), avail);
+        const uint32_t rank = __popc(F & lt);
+        if (fr && rank < take) {
+          const uint64_t local = next + rank;
+          const uint4 r = rec[local];  // first data vertex, query size | flags, query offset, data graph
+          if (r.w >= skip_below && !(r.y & 0x200u)) {
+            const uint64_t c0 = masks[local];
+            if (c0) {
+              w.pinfo[lane] = make_uint4(r.x, r.z | ((r.y & 0x100u) ? 0x80000000u : 0u), static_cast<uint32_t>(local), r.y & 0xFFu);
+              w.pcand[lane] = c0;
+              w.pcnt[lane] = 0;
+              w.pref[lane] = 1;
+              fr = false;
+            } else {
+              counts[slot0 + local] = 0;  // no candidate for the first query vertex
+            }
+          }
+        }
+        next += take;
+        F = __ballot_sync(kAll, fr);
+      }
+      __syncwarp();
+    }
+    // ---- one round at level L: this lane's source entry (L = 0: pair slot)
+    const uint32_t head = w.head[L], tail = w.tail[L];
+    uint64_t cand;
+    if (L == 0) cand = w.pcand[lane];
+    else cand = head + lane < tail ? w.ecand[head + lane] : 0ull;
+    const uint32_t c = __popcll(cand);
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kAll, incl, o);
+      if (lane >= static_cast<unsigned>(o)) incl += y;
+    }
+    const uint32_t excl = incl - c;
+    const uint32_t total = __shfl_sync(kAll, incl, 31);
+    if (total) {
+      const uint32_t nitems = total < 32u ? total : 32u;
+      // the owner of item `lane`: the first source lane whose inclusive
+      // count exceeds it (binary search over the non-decreasing counts)
+      uint32_t o = 0;
+#pragma unroll
+      for (uint32_t step = 16; step; step >>= 1) {
+        const uint32_t v = __shfl_sync(kAll, incl, o + step - 1u);
+        if (v <= lane) o += step;
+      }
+      o = o < 31u ? o : 31u;
+      const uint32_t oexcl = __shfl_sync(kAll, excl, o), oincl = __shfl_sync(kAll, incl, o);
+      const uint64_t ocand = __shfl_sync(kAll, cand, o);
+      const bool item = lane < nitems;
+      bool child = false, exhausted = false;
+      uint64_t nx = 0;
+      uint32_t p = 0, t = 0;
+      if (item) {
+        t = nth_set64(ocand, lane - oexcl);
+        const bool last_of_owner = lane + 1u == (oincl < nitems ? oincl : nitems);
+        uint32_t meta = 0;
+        if (L == 0) {
+          p = o;
+        } else {
+          meta = w.emeta[head + o];
+          p = meta & 31u;
+        }
+        if (last_of_owner) {  // the owner's candidates up to t are taken
+          const uint64_t left = ocand & ~((2ull << t) - 1ull);
+          if (L == 0) w.pcand[o] = left;
+          else w.ecand[head + o] = left;
+          exhausted = left == 0;
+        }
+        const uint4 pi = w.pinfo[p];
+        const uint32_t s = pi.x, sv = pi.y, local = pi.z, n = pi.w;
+        const uint64_t* selp = ((sv >> 31) ? qsel_id : qsel) + (sv & 0x7FFFFFFFu);
+        const uint64_t sl = selp[L + 1];
+        uint64_t b = masks[(L + 1u) * static_cast<uint32_t>(count) + local];
+        uint64_t used = 0;
+        if (L) {  // constraints of the vertices placed at levels L-1 .. 0
+          uint32_t m = meta;
+          for (int i = static_cast<int>(L) - 1;; --i) {
+            const uint32_t ti = (m >> 5) & 63u;
+            b &= ~(dadj[static_cast<uint64_t>(s + ti) * DAW] ^ (0ull - ((sl >> i) & 1ull)));
+            if (EXACT) used |= 1ull << ti;
+            if (i == 0) break;
+            m = w.emeta[m >> 11];
+          }
+        }
+        const uint64_t rw = dadj[static_cast<uint64_t>(s + t) * DAW];
+        nx = b & ~(rw ^ (0ull - ((sl >> L) & 1ull)));
+        if (EXACT) nx &= ~(used | (1ull << t));
+        if (!(find_first && w.pcnt[p])) {
+          if (L + 1u == n - 1u) {
+            if (nx) atomicAdd(&w.pcnt[p], static_cast<unsigned long long>(__popcll(nx)));
+          } else {
+            child = nx != 0;
+          }
+        }
+      }
+      // children at level L + 1, in lane order
+      const unsigned cb = __ballot_sync(kAll, child);
+      const uint32_t at = w.tail[L + 1];
+      if (child) {
+        const uint32_t pos = at + __popc(cb & lt);
+        if (pos < kFrontPool) {  // always true: the level bounds above sum to kFrontPool
+          w.ecand[pos] = nx;
+          w.emeta[pos] = p | (t << 5) | ((L ? head + o : 0u) << 11);
+          atomicAdd(&w.pref[p], 1u);
+        }
+      }
+      __syncwarp();
+      if (lane == 0 && cb) {
+        const uint32_t nt = min(at + static_cast<uint32_t>(__popc(cb)), kFrontPool);
+        w.tail[L + 1] = static_cast<uint16_t>(nt);
+        w.head[L + 2] = w.tail[L + 2] = static_cast<uint16_t>(nt);  // level L+2 is empty
+      }
+      // entries used up in this round release their pair; the last one ends it
+      if (exhausted && atomicSub(&w.pref[p], 1u) == 1u) {
+        unsigned long long cn = w.pcnt[p];
+        if (find_first && cn) cn = 1;
+        counts[slot0 + w.pinfo[p].z] = cn;
+        my_total += cn;
+        w.pinfo[p].z = kFrontFree;
+      }
+      if (L) {  // the used-up entries are a prefix of the level
+        const unsigned gone = __ballot_sync(kAll, incl <= 32u);
+        const uint32_t lead = gone == kAll ? 32u : static_cast<uint32_t>(__ffs(~gone) - 1);
+        if (lane == 0) w.head[L] = static_cast<uint16_t>(head + lead < tail ? head + lead : tail);
+      }
+      __syncwarp();
+    }
+    // ---- next level (warp-uniform)
+    const bool left = L ? w.head[L] < w.tail[L] : __any_sync(kAll, w.pcand[lane] != 0);
+    const uint32_t waiting = w.tail[L + 1] - w.head[L + 1];
+    const uint32_t thr = L + 1u <= kFrontDeep ? 32u : 1u;
+    if (waiting && (waiting >= thr || !left)) {
+      ++L;
+      continue;
+    }
+    if (!left) {
+      if (L) {
+        const uint16_t start = L == 1 ? 0 : w.tail[L - 1];
+        __syncwarp();
+        if (lane == 0) w.head[L] = w.tail[L] = w.head[L + 1] = w.tail[L + 1] = start;
+        __syncwarp();
+        --L;
+      } else if (!more) {
+        break;  // no pair in flight and no work left
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) my_total += __shfl_xor_sync(0xFFFFFFFFu, my_total, o);
+  if (lane == 0 && my_total) atomicAdd(d_total, static_cast<unsigned long long>(my_total));
+}
+
 }  // namespace
 
 int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const Candidates* c, Gmcr* m, int find_first,
@@ -880,14 +1120,27 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
     const uint64_t chunk = std::min<uint64_t>(m->total, static_cast<uint64_t>(tn.mask_chunk_slots) << 20);
     void* mbuf = nullptr;
     rc = dev_alloc(q, &mbuf, 8ull * kPhaseLevels * chunk + 16ull * chunk);
-    const size_t smem = static_cast<size_t>(kPhaseLevels) * kPhaseThreads * (2 * 8 + 1);
-    // the kernel for this batch's adjacency-row width and profile
+    // the kernel for this batch's adjacency-row width and profile: the
+    // per-lane DFS machine, or the warp-cooperative frontier join
+    const bool frontier = tn.join_kernel == 1;
+    const size_t smem = frontier ? sizeof(FrontWarp) * kFrontWarps
+                                 : static_cast<size_t>(kPhaseLevels) * kPhaseThreads * (2 * 8 + 1);
+    const unsigned block = frontier ? kFrontWarps * 32u : kPhaseThreads;
     void (*join_kernel)(const uint64_t*, const uint4*, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const uint64_t*,
                         uint32_t, int, uint32_t, unsigned long long*, uint64_t*, unsigned long long*) = nullptr;
     switch (data->adj_words) {
-      case 1: join_kernel = exact ? k_join_masks<true, 1> : k_join_masks<false, 1>; break;
-      case 2: join_kernel = exact ? k_join_masks<true, 2> : k_join_masks<false, 2>; break;
-      default: join_kernel = exact ? k_join_masks<true, 4> : k_join_masks<false, 4>; break;
+      case 1:
+        join_kernel = frontier ? (exact ? k_join_frontier<true, 1> : k_join_frontier<false, 1>)
+                               : (exact ? k_join_masks<true, 1> : k_join_masks<false, 1>);
+        break;
+      case 2:
+        join_kernel = frontier ? (exact ? k_join_frontier<true, 2> : k_join_frontier<false, 2>)
+                               : (exact ? k_join_masks<true, 2> : k_join_masks<false, 2>);
+        break;
+      default:
+        join_kernel = frontier ? (exact ? k_join_frontier<true, 4> : k_join_frontier<false, 4>)
+                               : (exact ? k_join_masks<true, 4> : k_join_masks<false, 4>);
+        break;
     }
     if (!rc) rc = allow_max_dynamic_smem(reinterpret_cast<const void*>(join_kernel), q->device);
     for (uint64_t slot0 = 0; slot0 < m->total && !rc; slot0 += chunk) {
@@ -906,9 +1159,9 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device);
         const unsigned grid = static_cast<unsigned>(sms) * tn.join_blocks_per_sm;
-        join_kernel<<<grid, kPhaseThreads, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id, data->adj,
-                                                              skip, find_first, tn.join_chunk, ctr, m->counts, tot);
-        rc = check_launch(q, "k_join_masks");
+        join_kernel<<<grid, block, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id, data->adj, skip,
+                                                      find_first, tn.join_chunk, ctr, m->counts, tot);
+        rc = check_launch(q, frontier ? "k_join_frontier" : "k_join_masks");
       }
     }
     dev_free(q, mbuf);

@@ -48,10 +48,12 @@ def run_plain(qh, dh, R, profile, find_first, wg=128, keep=False):
     return hist
 
 
-def run_batched(qh, dh, R, profile, find_first, wg=128, keep_bits=False):
+def run_batched(qh, dh, R, profile, find_first, wg=128, keep_bits=False, join_kernel=0):
     """keep_bits: the bitset route (final bitset materialised); otherwise the
-    plane route, which never writes the bitset."""
+    plane route, which never writes the bitset.  join_kernel: 0 the per-lane
+    DFS machine, 1 the warp-cooperative frontier join."""
     queue = sb.Queue(0, profile=profile, join_work_group_size=wg)
+    queue.set_tuning(join_kernel=join_kernel)
     qg, dg = sb.createDeviceCSRGraph(queue, qh), sb.createDeviceCSRGraph(queue, dh)
     cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes) if keep_bits else None
     gm = sb.GMCR(queue)
@@ -186,6 +188,27 @@ def test_symmetry_stress_small(prof):
     _check(run_plain(qh, dh, 3, prof, False), ref, "plain")
     _check(run_both_batched(qh, dh, 3, prof, False), ref, "batched")
     assert ref["per_pair"].max() >= 12  # automorphic patterns give many embeddings
+
+
+@pytest.mark.parametrize("prof", DEVICE_PROFILES)
+@pytest.mark.parametrize("ff", [False, True])
+def test_frontier_join_matches_oracle(prof, ff):
+    """The warp-cooperative frontier join (join_kernel=1) gives the oracle's
+    GMCR and per-pair counts: drug-like pairs, queries over 16 vertices and
+    molecules over 64 atoms (both take the generic kernel), and automorphic
+    queries on ring-rich molecules (thousands of embeddings per pair, the
+    deepest frontier levels)."""
+    cases = [
+        (sb.generate_molecules(1500, 10, 60, seed=5101), sb.generate_queries(120, 3, 24, seed=5102, skew_lo=6, skew_hi=15), 6),
+        (sb.generate_molecules(400, 6, 120, seed=5103, kind=1, median=30), sb.generate_queries(30, 3, 14, seed=5104), 4),
+        (sb.generate_molecules(200, 12, 50, seed=5105, kind=2), sb.generate_queries(16, 4, 12, seed=5106, kind=3), 3),
+    ]
+    for i, (dh, qh, R) in enumerate(cases):
+        ref = _oracle(qh, dh, R, prof, ff)
+        out = run_batched(qh, dh, R, prof, ff, join_kernel=1)
+        _check(out, ref, f"case {i}")
+        assert np.array_equal(out["per_pair"], run_batched(qh, dh, R, prof, ff)["per_pair"]), f"case {i}"
+    assert ref["per_pair"].max() >= (1 if ff else 12)
 
 
 def test_edge_inputs():

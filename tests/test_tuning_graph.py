@@ -55,7 +55,8 @@ def test_autotune_keeps_results_and_sets_the_queue():
     assert t["ms_join"] > 0 and t["ms_join_default"] > 0
     assert t["ms_join"] <= t["ms_join_default"] * 1.05
     got = queue.get_tuning()
-    for k in ("join_blocks_per_sm", "join_chunk", "overflow_blocks", "overflow_serial", "mask_chunk_slots", "overflow_split"):
+    for k in ("join_blocks_per_sm", "join_chunk", "overflow_blocks", "overflow_serial", "mask_chunk_slots", "overflow_split",
+              "join_kernel"):
         assert got[k] == t[k]
     after = sb.match_batched(queue, qg, dg, R, False, None, sb.GMCR(queue))
     assert after["total_matches"] == base["total_matches"]
@@ -68,5 +69,13 @@ def test_autotune_keeps_results_and_sets_the_queue():
         assert r["total_matches"] == base["total_matches"]
         f = sb.match_batched(queue, qg, dg, R, True, None, gm)
         assert f["total_matches"] == base_ff["total_matches"]
+    # the frontier join under graph replay
+    queue.set_tuning(join_kernel=1, join_blocks_per_sm=3, join_chunk=4, mask_chunk_slots=8, overflow_split=16)
+    gm = sb.GMCR(queue)
+    for _ in range(3):
+        r = sb.match_batched(queue, qg, dg, R, False, None, gm, graph=True)
+        assert r["total_matches"] == base["total_matches"]
     with pytest.raises(sb.SigmoError):
         queue.set_tuning(join_blocks_per_sm=9)
+    with pytest.raises(sb.SigmoError):
+        queue.set_tuning(join_kernel=2)
