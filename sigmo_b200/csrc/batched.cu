@@ -114,7 +114,17 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
                    [&](uint32_t l, uint32_t c) { vprog.push_back(static_cast<uint16_t>(thr_idx[(r * 16 + l) * 16 + c])); });
     voff[v + 1] = static_cast<uint32_t>(vprog.size());
   }
+  // sort key: the first four plane ids packed high to low (missing ones 0:
+  // only position 0, the label plane, can hold id 0, so a shorter program
+  // still sorts first); ties fall back to the full comparison
+  std::vector<uint64_t> pkey(Qn);
+  for (uint64_t v = 0; v < Qn; ++v) {
+    uint64_t k = 0;
+    for (uint32_t i = 0; i < 4; ++i) k = (k << 16) | (voff[v] + i < voff[v + 1] ? vprog[voff[v] + i] : 0u);
+    pkey[v] = k;
+  }
   auto prog_less = [&](uint32_t a, uint32_t b2) {
+    if (pkey[a] != pkey[b2]) return pkey[a] < pkey[b2];
     return std::lexicographical_compare(vprog.begin() + voff[a], vprog.begin() + voff[a + 1], vprog.begin() + voff[b2],
                                         vprog.begin() + voff[b2 + 1]);
   };
@@ -470,17 +480,22 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   if (!rc) rc = launch_gmcr_from_admit(q, query, data, admit, adm_counts, m, !run.capture, run.capture ? m->total : 0);
   if (!rc) rc = mark(3);
   const bool literal = !rc && L && m->total;
+  uint32_t reserve = 0;
   if (literal) {
     // REF_PTX: graphs starting below vertex 256 keep the reference's live
     // `visited` bitset, so they take the literal join on the bitset words it
-    // reads.  That runs on the side stream, overlapping the fast join.
-    const cudaStream_t main_stream = q->stream;
-    if (cudaEventRecord(q->ev_fork, main_stream) != cudaSuccess || cudaStreamWaitEvent(q->side, q->ev_fork, 0) != cudaSuccess)
-      rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
-    q->stream = q->side;
+    // reads.  The words are computed here (a few KB per query vertex); the
+    // literal join then runs on the side stream, overlapping the fast join,
+    // which leaves one CTA slot per literal block free so that the literal
+    // join does not wait behind its persistent CTAs.
     for (uint32_t r = 0; r < R && !rc; ++r)
       rc = launch_sig_planes(q, dsig + static_cast<uint64_t>(r) * N, N, Wlp, lplanes + static_cast<uint64_t>(r) * 16 * 4 * Wlp);
     if (!rc) rc = launch_fused_filter_raw(q, query->node_labels, pp.qsig_all, Qn, data->node_labels, N, lplanes, Wlp, R, lbits);
+    const cudaStream_t main_stream = q->stream;
+    if (!rc && (cudaEventRecord(q->ev_fork, main_stream) != cudaSuccess || cudaStreamWaitEvent(q->side, q->ev_fork, 0) != cudaSuccess))
+      rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
+    q->stream = q->side;
+    reserve = std::min<uint32_t>(L, 148u);
     Candidates view;
     view.q = q;
     view.rows = Qn;
@@ -492,8 +507,8 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
     q->stream = main_stream;
   }
   if (!rc)
-    rc = rp ? launch_join_fast_planes(q, query, data, pp, rp->planes, rp->rows, d_rprog, m, find_first, d_total)
-            : launch_join_fast_planes(q, query, data, pp, planes, pp.K, pp.prog, m, find_first, d_total);
+    rc = rp ? launch_join_fast_planes(q, query, data, pp, rp->planes, rp->rows, d_rprog, m, find_first, d_total, reserve)
+            : launch_join_fast_planes(q, query, data, pp, planes, pp.K, pp.prog, m, find_first, d_total, reserve);
   // join the side stream back before the scratch is released and the total read
   if (cudaEventRecord(q->ev_join, q->side) != cudaSuccess || cudaStreamWaitEvent(q->stream, q->ev_join, 0) != cudaSuccess)
     rc = rc ? rc : fail(SIGMO_ERR_CUDA, "stream join failed");

@@ -205,8 +205,10 @@ int launch_join_wildcard(Queue* q, const Graph* query, const Graph* data, const 
                          uint64_t* d_total);
 // planes: [graph / 32][planes_rows][AW][32]; prog: the class programs as
 // row indices into it (pp.prog for the per-batch planes).
+// reserve: persistent join CTA slots left free for a kernel running beside it
 int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, const PlaneProgram& pp, const uint64_t* planes,
-                            uint32_t planes_rows, const uint16_t* prog, Gmcr* m, int find_first, uint64_t* d_total);
+                            uint32_t planes_rows, const uint16_t* prog, Gmcr* m, int find_first, uint64_t* d_total,
+                            uint32_t reserve = 0);
 int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const uint32_t* NE, const uint32_t* cls, Gmcr* m,
                         bool sync_total, uint64_t capacity_hint);
 int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,

@@ -1099,7 +1099,8 @@ int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Cand
 }
 
 int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, const PlaneProgram& pp, const uint64_t* planes,
-                            uint32_t planes_rows, const uint16_t* prog, Gmcr* m, int find_first, uint64_t* d_total) {
+                            uint32_t planes_rows, const uint16_t* prog, Gmcr* m, int find_first, uint64_t* d_total,
+                            uint32_t reserve) {
   if (!m->total) return SIGMO_OK;
   if (query->max_nodes > kMaxQueryNodes)
     return fail(SIGMO_ERR_DOMAIN, "query graphs of up to %u vertices are supported (largest: %u)", kMaxQueryNodes, query->max_nodes);
@@ -1158,7 +1159,9 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
         SIGMO_CUDA_TRY(cudaMemsetAsync(ctr, 0, 8, q->stream));
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device);
-        const unsigned grid = static_cast<unsigned>(sms) * tn.join_blocks_per_sm;
+        // persistent CTAs; `reserve` slots stay free for a kernel running beside them
+        const unsigned full = static_cast<unsigned>(sms) * tn.join_blocks_per_sm;
+        const unsigned grid = full > reserve + static_cast<unsigned>(sms) ? full - reserve : full;
         join_kernel<<<grid, block, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id, data->adj, skip,
                                                       find_first, tn.join_chunk, ctr, m->counts, tot);
         rc = check_launch(q, frontier ? "k_join_frontier" : "k_join_masks");
