@@ -114,7 +114,11 @@ int finish_graph(Graph* g) {
   }
   g->max_nodes = mx;
   g->low_offset_graphs = low;
-  return launch_graph_derive(g);
+  SIGMO_TRY(launch_graph_derive(g));
+  // lets work on another stream wait for this graph alone
+  if (!g->ready) SIGMO_CUDA_TRY(cudaEventCreateWithFlags(&g->ready, cudaEventDisableTiming));
+  SIGMO_CUDA_TRY(cudaEventRecord(g->ready, g->q->stream));
+  return SIGMO_OK;
 }
 
 }  // namespace sigmo_b200
@@ -363,6 +367,7 @@ int sigmo_graph_destroy(sigmo_graph_t g) {
   dev_free(q, g->qsel);
   dev_free(q, g->qsel_id);
   release_plane_program(g);
+  if (g->ready) cudaEventDestroy(g->ready);
   delete g;
   return SIGMO_OK;
 }

@@ -58,6 +58,16 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   PlaneProgram& pp = query->pp;
   if (pp.valid && pp.R == R && pp.profile == q->opts.profile) return SIGMO_OK;
   free_program(q, &pp);
+  // The program's device work runs on the side stream after the query
+  // graph's own creation work only, so a data graph upload queued on the main
+  // stream meanwhile overlaps the host work below.
+  struct OnSide {
+    Queue* q;
+    cudaStream_t main;
+    ~OnSide() { q->stream = main; }
+  } on_side{q, q->stream};
+  if (query->ready) SIGMO_CUDA_TRY(cudaStreamWaitEvent(q->side, query->ready, 0));
+  q->stream = q->side;
   const uint64_t Qn = query->total_nodes;
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&pp.qsig_all), 8ull * (R ? R : 1) * (Qn ? Qn : 1)));
   SIGMO_TRY(launch_sig_all(q, query, R, pp.qsig_all));

@@ -114,6 +114,7 @@ struct Graph {
   std::vector<uint32_t> host_graph_offsets;  // host copy (sizes, dispatch)
   std::vector<uint64_t> label_hist;          // vertices per label (filled on first use, 256 entries)
   uint64_t stamp = 0;                        // unique per graph object (cache keys)
+  cudaEvent_t ready = nullptr;               // recorded after the creation work on the queue's stream
   PlaneProgram pp;                 // when this graph is the query side of a batched match
 };
 
