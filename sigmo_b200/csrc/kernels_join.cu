@@ -637,7 +637,8 @@ __global__ void __launch_bounds__(128) k_join_fast(
 // Two-phase join for pairs whose query has <= kPhaseLevels vertices.
 // Phase A (k_pair_masks): per slot of a chunk and per level j, the candidate
 // set of the query vertex placed at level j = AND of its class's plane program
-// for the slot's data graph, stored [level][slot-in-chunk] (coalesced).
+// for the slot's data graph, stored [slot-in-chunk][level] (coalesced: one
+// 128-byte line per slot, so a pair's later levels hit in cache).
 // Phase B (k_join_masks): the DFS as a flat per-lane state machine whose pair
 // setup is just the load of those masks, with the per-level state in shared
 // memory ([level][thread]).  Trying a candidate t at level k is O(1):
@@ -656,8 +657,8 @@ __global__ void __launch_bounds__(256) k_pair_masks(
     unsigned long long* __restrict__ overflow_len, uint64_t* __restrict__ counts) {
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count * kPhaseLevels; i += stride) {
-    const uint64_t local = i % count;  // slot within the chunk (fastest), then level
-    const uint32_t j = static_cast<uint32_t>(i / count);
+    const uint64_t local = i / kPhaseLevels;  // slot within the chunk, then level (fastest)
+    const uint32_t j = static_cast<uint32_t>(i % kPhaseLevels);
     const uint64_t slot = slot0 + local;
     const uint32_t qg = indices[slot];
     const uint32_t qoff = qgoff[qg], n = qgoff[qg + 1] - qoff;
@@ -681,7 +682,7 @@ __global__ void __launch_bounds__(256) k_pair_masks(
     uint64_t m = ~0ull;
     const uint32_t e1 = prog_off[c + 1];
     for (uint32_t e = prog_off[c]; e < e1; ++e) m &= base[static_cast<uint64_t>(prog[e]) * AW * 32];
-    masks[static_cast<uint64_t>(j) * count + local] = m;
+    masks[local * kPhaseLevels + j] = m;
   }
 }
 
@@ -731,8 +732,8 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
       if (r.y & 0x200u) continue;  // in the overflow list (generic kernel)
       s = r.x;
       selp = ((r.y & 0x100u) ? qsel_id : qsel) + r.z;
-      AT(cand, 0) = masks[local];
-      AT(base, 1) = masks[count + local];
+      AT(cand, 0) = masks[local * kPhaseLevels];
+      AT(base, 1) = masks[local * kPhaseLevels + 1];
       used = 0;
       cnt = 0;
       k = 0;
@@ -761,7 +762,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
     if (EXACT) used |= 1ull << t;
     AT(cand, k + 1) = nx;
     const uint64_t sl2 = selp[k + 2];
-    uint64_t b2 = masks[static_cast<uint64_t>(k + 2) * count + local] & ~(rw ^ (0ull - ((sl2 >> k) & 1ull)));
+    uint64_t b2 = masks[local * kPhaseLevels + k + 2] & ~(rw ^ (0ull - ((sl2 >> k) & 1ull)));
     for (int i = 0; i < k; ++i) b2 &= ~(dadj[static_cast<uint64_t>(s + AT(pk, i)) * DAW] ^ (0ull - ((sl2 >> i) & 1ull)));
     AT(base, k + 2) = b2;
     ++k;
@@ -864,7 +865,7 @@ __global__ void __launch_bounds__(kFrontWarps * 32, 3) k_join_frontier(
           const uint64_t local = next + rank;
           const uint4 r = rec[local];  // first data vertex, query size | flags, query offset, data graph
           if (r.w >= skip_below && !(r.y & 0x200u)) {
-            const uint64_t c0 = masks[local];
+            const uint64_t c0 = masks[local * kPhaseLevels];
             if (c0) {
               w.pinfo[lane] = make_uint4(r.x, r.z | ((r.y & 0x100u) ? 0x80000000u : 0u), static_cast<uint32_t>(local), r.y & 0xFFu);
               w.pcand[lane] = c0;
@@ -932,7 +933,7 @@ __global__ void __launch_bounds__(kFrontWarps * 32, 3) k_join_frontier(
         const uint32_t s = pi.x, sv = pi.y, local = pi.z, n = pi.w;
         const uint64_t* selp = ((sv >> 31) ? qsel_id : qsel) + (sv & 0x7FFFFFFFu);
         const uint64_t sl = selp[L + 1];
-        uint64_t b = masks[(L + 1u) * static_cast<uint32_t>(count) + local];
+        uint64_t b = masks[static_cast<uint64_t>(local) * kPhaseLevels + L + 1u];
         uint64_t used = 0;
         if (L) {  // constraints of the vertices placed at levels L-1 .. 0
           uint32_t m = meta;
