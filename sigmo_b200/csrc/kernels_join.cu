@@ -640,8 +640,9 @@ __global__ void __launch_bounds__(128) k_join_fast(
 // for the slot's data graph, stored [slot-in-chunk][level] (coalesced: one
 // 128-byte line per slot, so a pair's later levels hit in cache).
 // Phase B (k_join_masks): the DFS as a flat per-lane state machine whose pair
-// setup is just the load of those masks, with the per-level state in shared
-// memory ([level][thread]).  Trying a candidate t at level k is O(1):
+// setup is just the load of those masks (issued one pair ahead, so the DRAM
+// latency of a refill overlaps the current pair's DFS), with the per-level
+// state in shared memory ([level][thread]).  Trying a candidate t at level k is O(1):
 // next = base[k+1] & (row(t) or ~row(t)) [& ~used]; base[k+2] is computed
 // once per descent.
 constexpr uint32_t kPhaseLevels = 16;
@@ -706,6 +707,30 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
   uint64_t used = 0;
   int k = -1;
   bool have = false;
+  // the next slot's record and first two level masks, loaded one pair ahead
+  uint4 pr = make_uint4(0, 0, 0, 0);
+  uint64_t pm0 = 0, pm1 = 0, plocal = 0;
+  bool pre = false;
+  auto fetch = [&]() {
+    pre = false;
+    if (next >= end) {
+      const unsigned am = __activemask();
+      const unsigned leader = __ffs(am) - 1;
+      const unsigned rank = __popc(am & ((1u << lane) - 1u));
+      unsigned long long b = 0;
+      if (lane == leader) b = atomicAdd(cursor, static_cast<unsigned long long>(__popc(am)) * kChunk);
+      b = __shfl_sync(am, b, leader);
+      next = b + static_cast<uint64_t>(rank) * kChunk;
+      end = next + kChunk < count ? next + kChunk : count;
+      if (next >= count) return;
+    }
+    plocal = next++;
+    pr = rec[plocal];
+    pm0 = masks[plocal * kPhaseLevels];
+    pm1 = masks[plocal * kPhaseLevels + 1];
+    pre = true;
+  };
+  fetch();
   for (;;) {
     if (k < 0) {
       if (have) {
@@ -714,26 +739,18 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
         my_total += cnt;
         have = false;
       }
-      if (next >= end) {
-        const unsigned am = __activemask();
-        const unsigned leader = __ffs(am) - 1;
-        const unsigned rank = __popc(am & ((1u << lane) - 1u));
-        unsigned long long b = 0;
-        if (lane == leader) b = atomicAdd(cursor, static_cast<unsigned long long>(__popc(am)) * kChunk);
-        b = __shfl_sync(am, b, leader);
-        next = b + static_cast<uint64_t>(rank) * kChunk;
-        end = next + kChunk < count ? next + kChunk : count;
-        if (next >= count) break;
-      }
-      local = next++;
-      const uint4 r = rec[local];  // first data vertex, query size | order flag, query offset, data graph
+      if (!pre) break;
+      local = plocal;
+      const uint4 r = pr;  // first data vertex, query size | order flag, query offset, data graph
+      const uint64_t m0 = pm0, m1 = pm1;
+      fetch();
       if (r.w < skip_below) continue;
       n = r.y & 0xFFu;
       if (r.y & 0x200u) continue;  // in the overflow list (generic kernel)
       s = r.x;
       selp = ((r.y & 0x100u) ? qsel_id : qsel) + r.z;
-      AT(cand, 0) = masks[local * kPhaseLevels];
-      AT(base, 1) = masks[local * kPhaseLevels + 1];
+      AT(cand, 0) = m0;
+      AT(base, 1) = m1;
       used = 0;
       cnt = 0;
       k = 0;
