@@ -278,7 +278,23 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
           for (int w = 0; w < AW; ++w) m[w] = ~0ull;
           bool any = true;
           const uint32_t k1 = prog_off[c + 1];
-          for (uint32_t k = prog_off[c]; k < k1; ++k) {
+          // two planes per step between the warp votes
+          uint32_t k = prog_off[c];
+          bool live = true;
+          for (; k + 2 <= k1; k += 2) {
+            const uint32_t off0 = static_cast<uint32_t>(prog[k]) * kRow, off1 = static_cast<uint32_t>(prog[k + 1]) * kRow;
+            any = false;
+#pragma unroll
+            for (int w = 0; w < AW; ++w) {
+              m[w] &= tl[off0 + 32 * w] & tl[off1 + 32 * w];
+              any |= m[w] != 0;
+            }
+            if (!__any_sync(0xFFFFFFFFu, any)) {
+              live = false;
+              break;
+            }
+          }
+          if (live && k < k1) {
             const uint32_t off = static_cast<uint32_t>(prog[k]) * kRow;
             any = false;
 #pragma unroll
@@ -286,7 +302,6 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
               m[w] &= tl[off + 32 * w];
               any |= m[w] != 0;
             }
-            if (!__any_sync(0xFFFFFFFFu, any)) break;
           }
           word = __ballot_sync(0xFFFFFFFFu, any);
           if (lane == 0) {
