@@ -491,6 +491,7 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   if (!rc) rc = mark(3);
   const bool literal = !rc && L && m->total;
   uint32_t reserve = 0;
+  bool forked = false;  // the side stream joined this call's work
   if (literal) {
     // REF_PTX: graphs starting below vertex 256 keep the reference's live
     // `visited` bitset, so they take the literal join on the bitset words it
@@ -504,6 +505,7 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
     const cudaStream_t main_stream = q->stream;
     if (!rc && (cudaEventRecord(q->ev_fork, main_stream) != cudaSuccess || cudaStreamWaitEvent(q->side, q->ev_fork, 0) != cudaSuccess))
       rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
+    forked = !rc;
     q->stream = q->side;
     reserve = std::min<uint32_t>(L, 148u);
     Candidates view;
@@ -519,8 +521,10 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   if (!rc)
     rc = rp ? launch_join_fast_planes(q, query, data, pp, rp->planes, rp->rows, d_rprog, m, find_first, d_total, reserve)
             : launch_join_fast_planes(q, query, data, pp, planes, pp.K, pp.prog, m, find_first, d_total, reserve);
-  // join the side stream back before the scratch is released and the total read
-  if (cudaEventRecord(q->ev_join, q->side) != cudaSuccess || cudaStreamWaitEvent(q->stream, q->ev_join, 0) != cudaSuccess)
+  // join the side stream back before the scratch is released and the total
+  // read (only when this call forked it: a CUDA-graph capture may wait only
+  // on events of streams that joined the capture)
+  if (forked && (cudaEventRecord(q->ev_join, q->side) != cudaSuccess || cudaStreamWaitEvent(q->stream, q->ev_join, 0) != cudaSuccess))
     rc = rc ? rc : fail(SIGMO_ERR_CUDA, "stream join failed");
   dev_free(q, buf);
   return rc;

@@ -128,3 +128,23 @@ def test_serving_rejects_bad_requests():
         assert ei.value.code == 4
         with pytest.raises(sb.SigmoError):
             srv.wait(12345)
+
+
+def test_serving_exact_profile_heavy_tail_against_oracle():
+    """EXACT profile, find-all, on a database with molecules over 64 atoms and
+    requests with queries over 16 vertices (both take the generic join):
+    per-query totals equal the oracle's per-pair counts summed per query."""
+    db = sb.generate_molecules(600, 6, 110, seed=931, kind=1, median=30)
+    assert int(db.sizes().max()) > 64
+    reqs = [sb.generate_queries(6, 3, 20, seed=932 + i, skew_lo=10, skew_hi=20) for i in range(3)]
+    assert max(int(q.sizes().max()) for q in reqs) > 16
+    with sb.Server(db, profile="exact", iterations=R, find_first=False, max_inflight=2, max_batch_queries=12,
+                   batch_window_us=100_000) as srv:
+        out = _run_all(srv, reqs, pairs=False)
+    for (r, m, tot, _), q in zip(out, reqs):
+        assert r["status"] == 0
+        ref = oracle.run_pipeline(q, db, R, oracle.EXACT, False)
+        per_q = np.zeros(q.num_graphs, np.uint64)
+        np.add.at(per_q, ref["indices"].astype(np.int64), ref["per_pair"].astype(np.uint64))
+        assert np.array_equal(tot, per_q)
+        assert r["total_matches"] == int(per_q.sum())

@@ -79,3 +79,17 @@ def test_autotune_keeps_results_and_sets_the_queue():
         queue.set_tuning(join_blocks_per_sm=9)
     with pytest.raises(sb.SigmoError):
         queue.set_tuning(join_kernel=2)
+
+
+def test_graph_mode_exact_profile():
+    """Graph replay under the EXACT profile equals the oracle on every replay."""
+    queue = sb.Queue(0, profile=oracle.EXACT)
+    d = sb.generate_molecules(1500, 10, 40, seed=1731)
+    q = sb.generate_queries(40, 3, 20, seed=1732, skew_lo=5, skew_hi=12)
+    qg, dg = sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)
+    want = oracle.run_pipeline(q, d, R, oracle.EXACT, False)
+    gm = sb.GMCR(queue)
+    for call in range(3):
+        r = sb.match_batched(queue, qg, dg, R, False, None, gm, graph=True)
+        assert r["total_matches"] == want["total"], f"call {call}"
+        assert np.array_equal(gm.getPairCounts(), want["per_pair"]), f"call {call}"
