@@ -377,6 +377,12 @@ def test_shards_keep_the_unsharded_results(ff):
         r = sb.match_batched(queue, qg, sg, 5, ff, None, gms)
         o, i = gms.getGMCR()
         assert np.array_equal(o.astype(np.int64), off[first:first + count + 1].astype(np.int64) - int(off[first]))
+        # CUDA-graph replay on the shard (shards with a base >= 256 have no literal join)
+        gmg = sb.GMCR(queue)
+        for _ in range(2):
+            rg = sb.match_batched(queue, qg, sg, 5, ff, None, gmg, graph=True)
+            assert rg["total_matches"] == r["total_matches"]
+            assert np.array_equal(gmg.getPairCounts(), gms.getPairCounts())
         tot += r["total_matches"]
         seg_idx.append(i)
         seg_cnt.append(gms.getPairCounts())

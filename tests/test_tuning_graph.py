@@ -93,3 +93,28 @@ def test_graph_mode_exact_profile():
         r = sb.match_batched(queue, qg, dg, R, False, None, gm, graph=True)
         assert r["total_matches"] == want["total"], f"call {call}"
         assert np.array_equal(gm.getPairCounts(), want["per_pair"]), f"call {call}"
+
+
+def test_no_admitted_pairs():
+    """A query batch that no molecule admits (labels the generator never
+    emits): zero pairs and zero matches in an ordinary call, under graph
+    replay, and as a serving request."""
+    d = sb.generate_molecules(800, 10, 30, seed=1741)
+    q = sb.io.parse("n#3 l#1 0 13 1 13 2 14 e#2 0 1 1 1 2 1\nn#2 l#1 0 15 1 15 e#1 0 1 1\n")
+    for prof in (oracle.REF_PTX, oracle.EXACT):
+        queue = sb.Queue(0, profile=prof)
+        qg, dg = sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)
+        gm = sb.GMCR(queue)
+        for ff in (False, True):
+            r = sb.match_batched(queue, qg, dg, R, ff, None, gm)
+            assert r["admitted_pairs"] == 0 and r["total_matches"] == 0
+            for _ in range(2):
+                r = sb.match_batched(queue, qg, dg, R, ff, None, gm, graph=True)
+                assert r["admitted_pairs"] == 0 and r["total_matches"] == 0
+    with sb.Server(d, iterations=R, find_first=True, max_inflight=1) as srv:
+        t = srv.submit(q, pairs=True)
+        res = srv.wait(t)
+        assert res["status"] == 0 and res["matched_pairs"] == 0 and res["total_matches"] == 0
+        m, tot = srv.query_totals(t, q.num_graphs)
+        assert not m.any() and not tot.any()
+        assert len(srv.pairs(t)[0]) == 0
