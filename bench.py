@@ -129,11 +129,24 @@ def make_workload(wl, rank=0):
     return q, d
 
 
+def use_all_host_threads():
+    """The oracle's OpenMP thread count = the host threads this process may
+    run on (torchrun sets OMP_NUM_THREADS=1 for its workers)."""
+    import oracle
+
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    oracle.lib().orc_set_num_threads(max(1, n))
+
+
 def cpu_baseline(q, d, wl, sample_mols, find_first, profile):
     """The oracle (CPU restatement of the reference) on the first
     `sample_mols` molecules x all queries, every host thread."""
     import oracle
 
+    use_all_host_threads()
     ds = d.slice(0, min(sample_mols, d.num_graphs))
     prof = {"ref-ptx": oracle.REF_PTX, "exact": oracle.EXACT}[profile]
     t0 = time.perf_counter()
@@ -595,6 +608,7 @@ def run_reference(args, rank, world, local):
     sample = min(args.cpu_sample // 5 if args.cpu_sample >= 5 else 1, d.num_graphs) or 1
     ds = d.slice(0, sample)
     pairs = q.num_graphs * ds.num_graphs
+    use_all_host_threads()
     for _ in range(max(args.warmup, 0)):
         oracle.run_pipeline(q, ds, wl["R"], prof, ff)
     times = []

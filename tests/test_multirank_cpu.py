@@ -95,3 +95,26 @@ def test_two_gloo_ranks_merge_shards_into_the_unsharded_result():
     for r in range(world):
         tot, merged, want_tot, want_per = got[r]
         assert tot == want_tot and merged == want_per
+
+
+@pytest.mark.timeout(300)
+def test_reference_arm_under_torchrun_prints_one_line_on_all_host_threads():
+    """`bench.py --impl reference` launched as two ranks: rank 0 alone runs
+    the oracle, on every host thread it may use (not torchrun's
+    OMP_NUM_THREADS=1), and prints one JSON line; the other rank exits 0."""
+    import json
+    import subprocess
+    import sys
+
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(_free_port()), "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1",
+           "--warmup", "0", "--workload", "drug1k", "--cpu-sample", "50"]
+    res = subprocess.run(cmd, cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), capture_output=True,
+                         text=True, timeout=280)
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [json.loads(x) for x in res.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    line = lines[0]
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+    assert line["cpu_baseline"]["cores"] == len(os.sched_getaffinity(0))
+    assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
