@@ -164,6 +164,10 @@ int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out
   if (st == cudaSuccess) st = cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking);
   if (st == cudaSuccess) st = cudaEventCreateWithFlags(&q->ev_fork, cudaEventDisableTiming);
   if (st == cudaSuccess) st = cudaEventCreateWithFlags(&q->ev_join, cudaEventDisableTiming);
+  if (st == cudaSuccess) st = cudaStreamCreateWithFlags(&q->aux, cudaStreamNonBlocking);
+  if (st == cudaSuccess) st = cudaEventCreateWithFlags(&q->ev_aux_fork, cudaEventDisableTiming);
+  if (st == cudaSuccess) st = cudaEventCreateWithFlags(&q->ev_aux_join, cudaEventDisableTiming);
+  for (int i = 0; i < 2 && st == cudaSuccess; ++i) st = cudaEventCreateWithFlags(&q->ev_masks[i], cudaEventDisableTiming);
   if (st == cudaSuccess) {
     // Keep freed stream-ordered allocations cached in the device's default pool
     // (per-call scratch is then reused instead of being remapped every call).
@@ -193,8 +197,16 @@ int sigmo_queue_destroy(sigmo_queue_t q) {
     cudaStreamSynchronize(q->side);
     cudaStreamDestroy(q->side);
   }
+  if (q->aux) {
+    cudaStreamSynchronize(q->aux);
+    cudaStreamDestroy(q->aux);
+  }
   if (q->ev_fork) cudaEventDestroy(q->ev_fork);
   if (q->ev_join) cudaEventDestroy(q->ev_join);
+  if (q->ev_aux_fork) cudaEventDestroy(q->ev_aux_fork);
+  if (q->ev_aux_join) cudaEventDestroy(q->ev_aux_join);
+  for (cudaEvent_t e : q->ev_masks)
+    if (e) cudaEventDestroy(e);
   if (q->ev_start) cudaEventDestroy(q->ev_start);
   if (q->ev_end) cudaEventDestroy(q->ev_end);
   if (q->pinned) cudaFreeHost(q->pinned);

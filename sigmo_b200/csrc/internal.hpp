@@ -42,6 +42,11 @@ struct Queue {
   void* pinned = nullptr;  // small pinned host buffer for scalar read-backs
   cudaStream_t side = nullptr;  // second stream for work that overlaps the main one
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // third stream: the join's odd chunks (level masks of one chunk overlap the
+  // join of the previous one), with its fork/join events and the events after
+  // each stream's last level-mask pass
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_aux_fork = nullptr, ev_aux_join = nullptr, ev_masks[2] = {nullptr, nullptr};
 };
 
 // A contiguous range of query graphs whose planes and classes fit one

@@ -1134,11 +1134,22 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
   // two-phase join, in chunks of slots, for the pairs of queries of <= 16
   // vertices and molecules of <= 64 atoms; the rest go to the overflow list
   int rc = SIGMO_OK;
+  bool two = false;
   {
     const sigmo_tuning& tn = q->tune;
     const uint64_t chunk = std::min<uint64_t>(m->total, static_cast<uint64_t>(tn.mask_chunk_slots) << 20);
-    void* mbuf = nullptr;
-    rc = dev_alloc(q, &mbuf, 8ull * kPhaseLevels * chunk + 16ull * chunk);
+    // several chunks: even ones on the main stream, odd ones on the aux
+    // stream, each stream with its own mask buffer and work cursor, so one
+    // chunk's level masks run beside the previous chunk's persistent join
+    two = m->total > chunk;
+    const size_t mbytes = 8ull * kPhaseLevels * chunk + 16ull * chunk;
+    void* mbuf[2] = {nullptr, nullptr};
+    rc = dev_alloc(q, &mbuf[0], mbytes);
+    if (!rc && two) rc = dev_alloc(q, &mbuf[1], mbytes);
+    const cudaStream_t streams[2] = {q->stream, q->aux};
+    if (!rc && two &&
+        (cudaEventRecord(q->ev_aux_fork, q->stream) != cudaSuccess || cudaStreamWaitEvent(q->aux, q->ev_aux_fork, 0) != cudaSuccess))
+      rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
     // the kernel for this batch's adjacency-row width and profile: the
     // per-lane DFS machine, or the warp-cooperative frontier join
     const bool frontier = tn.join_kernel == 1;
@@ -1162,37 +1173,46 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
         break;
     }
     if (!rc) rc = allow_max_dynamic_smem(reinterpret_cast<const void*>(join_kernel), q->device);
-    for (uint64_t slot0 = 0; slot0 < m->total && !rc; slot0 += chunk) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device);
+    uint64_t c = 0;
+    for (uint64_t slot0 = 0; slot0 < m->total && !rc; slot0 += chunk, ++c) {
       const uint64_t cnt = std::min<uint64_t>(chunk, m->total - slot0);
-      auto* masks = static_cast<uint64_t*>(mbuf);
+      const cudaStream_t st = streams[c & 1];
+      auto* masks = static_cast<uint64_t*>(mbuf[c & 1]);
       auto* recs = reinterpret_cast<uint4*>(masks + kPhaseLevels * chunk);
-      k_pair_masks<<<grid_for(cnt * kPhaseLevels, 256, 148u * 32u), 256, 0, q->stream>>>(
+      unsigned long long* cursor = ctr + ((c & 1) ? 3 : 0);
+      k_pair_masks<<<grid_for(cnt * kPhaseLevels, 256, 148u * 32u), 256, 0, st>>>(
           planes, planes_rows, data->adj_words, pp.prog_off, prog, pp.cls, query->graph_offsets, query->qorder, query->sym,
-          data->graph_offsets,
-          data->sym, m->indices, m->pair_graph, slot0, cnt, masks, recs, skip, overflow, ctr + 2, m->counts);
+          data->graph_offsets, data->sym, m->indices, m->pair_graph, slot0, cnt, masks, recs, skip, overflow, ctr + 2,
+          m->counts);
       rc = check_launch(q, "k_pair_masks");
-      if (!rc && slot0 + chunk >= m->total && cudaEventRecord(q->ev_fork, q->stream) != cudaSuccess)
-        rc = fail(SIGMO_ERR_CUDA, "event record failed");
+      if (!rc && cudaEventRecord(q->ev_masks[c & 1], st) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+      if (!rc && cudaMemsetAsync(cursor, 0, 8, st) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
       if (!rc) {
-        SIGMO_CUDA_TRY(cudaMemsetAsync(ctr, 0, 8, q->stream));
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, q->device);
         // persistent CTAs; `reserve` slots stay free for a kernel running beside them
         const unsigned full = static_cast<unsigned>(sms) * tn.join_blocks_per_sm;
         const unsigned grid = full > reserve + static_cast<unsigned>(sms) ? full - reserve : full;
-        join_kernel<<<grid, block, smem, q->stream>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id, data->adj, skip,
-                                                      find_first, tn.join_chunk, ctr, m->counts, tot);
+        join_kernel<<<grid, block, smem, st>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id, data->adj, skip,
+                                               find_first, tn.join_chunk, cursor, m->counts, tot);
         rc = check_launch(q, frontier ? "k_join_frontier" : "k_join_masks");
       }
     }
-    dev_free(q, mbuf);
+    // the aux stream joins the main one before its buffer is released
+    if (two && (cudaEventRecord(q->ev_aux_join, q->aux) != cudaSuccess ||
+                cudaStreamWaitEvent(q->stream, q->ev_aux_join, 0) != cudaSuccess))
+      rc = rc ? rc : fail(SIGMO_ERR_CUDA, "stream join failed");
+    dev_free(q, mbuf[0]);
+    dev_free(q, mbuf[1]);
   }
   const cudaStream_t main_stream = q->stream;
   const bool side = !q->tune.overflow_serial;
   if (!rc && side) {
-    // the overflow list is complete after the last Phase A: its pairs run on
-    // the side stream, overlapping Phase B (the caller joins the side stream)
-    if (cudaStreamWaitEvent(q->side, q->ev_fork, 0) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
+    // the overflow list is complete after the last Phase A of each stream: its
+    // pairs run on the side stream, overlapping Phase B
+    if (cudaStreamWaitEvent(q->side, q->ev_masks[0], 0) != cudaSuccess ||
+        (two && cudaStreamWaitEvent(q->side, q->ev_masks[1], 0) != cudaSuccess))
+      rc = fail(SIGMO_ERR_CUDA, "stream fork failed");
     q->stream = q->side;
   }
   if (!rc) {
