@@ -206,6 +206,31 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
             if (find_first) break;
             continue;
           }
+          if (small && qn + 1 == n && fr.idx == 0) {
+            // The last level in one step (graphs of <= 64 vertices).  Its
+            // candidates are distinct local bits, so placing one never hides a
+            // later one, and valid() does not read `visited`: the frame finds
+            // popc(candidates & valid & ~visited), sets the bits of those below
+            // vertex 256 (refbit gives none above), leaves mapping[n - 1] at the
+            // last one placed (the first under find-first, which stops there),
+            // then is used up -- what the candidate-by-candidate loop does.
+            const uint32_t sh = s & 31u;
+            const uint64_t lo = static_cast<uint64_t>(pc.w[qn][0]) | (static_cast<uint64_t>(pc.w[qn][1]) << 32);
+            const uint64_t cm = (lo >> sh) | (sh ? (static_cast<uint64_t>(pc.w[qn][2]) << (64u - sh)) : 0ull);
+            const uint64_t low = s >= 256u ? 0ull : (256u - s >= 64u ? ~0ull : ((1ull << (256u - s)) - 1ull));
+            uint64_t place = cm & vmask[qn] & ~visited;
+            if (place) {
+              if (find_first) place &= 0ull - place;
+              found += __popcll(place);
+              visited |= place & low;
+              mapping[qn] = s + 63u - static_cast<uint32_t>(__clzll(static_cast<long long>(place)));
+              if (find_first) break;
+            }
+            --top;
+            visited &= ~refbit(mapping[qn], s);
+            if (top == 1) visited = 0;
+            continue;
+          }
           if (fr.idx >= count_of(qn)) {
             --top;
             visited &= ~refbit(mapping[qn], s);
