@@ -32,6 +32,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -174,11 +175,13 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        # raw samples (the JSON line carries their summary); SIGMO_CLOCKS_DIR keeps them
+        out_dir = Path(os.environ.get("SIGMO_CLOCKS_DIR") or tempfile.gettempdir())
+        self.path = out_dir / f"sigmo_clocks_rank{index}_{os.getpid()}.csv"
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                                           "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
