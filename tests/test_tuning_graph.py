@@ -118,3 +118,25 @@ def test_no_admitted_pairs():
         m, tot = srv.query_totals(t, q.num_graphs)
         assert not m.any() and not tot.any()
         assert len(srv.pairs(t)[0]) == 0
+
+
+def test_several_mask_chunks_on_two_streams():
+    """More admitted slots than one level-mask chunk: chunks alternate between
+    two streams (each with its own mask buffer and work cursor).  Ordinary
+    calls and graph replays, with the overflow join after or beside the main
+    join, give the single-chunk per-pair counts."""
+    queue = sb.Queue(0)
+    d = sb.generate_molecules(40000, 10, 60, seed=20251)
+    q = sb.generate_queries(600, 3, 30, seed=20252, skew_lo=6, skew_hi=15)
+    qg, dg = sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)
+    gm = sb.GMCR(queue)
+    ref = sb.match_batched(queue, qg, dg, 6, False, None, gm)
+    assert ref["admitted_pairs"] > 2 * (1 << 20)  # three chunks of 2^20 slots
+    ref_counts = gm.getPairCounts()
+    for serial in (1, 0):
+        queue.set_tuning(mask_chunk_slots=1, overflow_serial=serial)
+        g2 = sb.GMCR(queue)
+        for graph in (False, True, True):
+            r = sb.match_batched(queue, qg, dg, 6, False, None, g2, graph=graph)
+            assert r["total_matches"] == ref["total_matches"], (serial, graph)
+            assert np.array_equal(g2.getPairCounts(), ref_counts), (serial, graph)
