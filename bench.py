@@ -438,8 +438,10 @@ def run_sigmo(args, rank, world, local):
             "algorithmic_bytes_per_launch": jb, "ms_per_launch": round(join_ms, 4),
             "warp_execution_efficiency": traffic_for("join", args.workload, "warp_execution_efficiency"),
             "active_warps_of_peak": traffic_for("join", args.workload, "active_warps_of_peak"),
-            "note": "DFS over admitted pairs: latency/issue-bound, no bandwidth roofline applies (ncu: threads per "
-                    "instruction / 32 and active warps above); the stage is "
+            "issue_active_of_peak": traffic_for("join", args.workload, "issue_active_of_peak"),
+            "note": "DFS over admitted pairs: latency-bound, no bandwidth roofline applies (ncu: threads per "
+                    "instruction / 32, active warps and issue-active fraction above; 92 % of its loads hit L2); "
+                    "the stage is "
                     f"{100 * join_ms / stages['ms_total']:.0f}% of the step"}
 
     # ---- the plain stage-per-launch form (same results, reference order) ----
