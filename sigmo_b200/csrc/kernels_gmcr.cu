@@ -113,9 +113,23 @@ __global__ void k_gmcr_fill(const uint32_t* __restrict__ admit, uint32_t GW, uin
   for (uint32_t gw = warp; gw < GW; gw += nwarps) {
     const uint32_t g = gw * 32u + lane;
     uint64_t cur = g < G ? offsets[g] : 0;
-    for (uint32_t q = 0; q < QG; ++q) {
+    uint32_t q = 0;
+    for (; q + 8 <= QG; q += 8) {  // eight admission words in flight
+      uint32_t a[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = admit[static_cast<uint64_t>(q + k) * GW + gw];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if ((a[k] >> lane) & 1u) {
+          if (cur < capacity) {
+            indices[cur] = q + k;
+            if (pair_graph) pair_graph[cur] = g;
+          }
+          ++cur;
+        }
+    }
+    for (; q < QG; ++q) {
       const uint32_t a = admit[static_cast<uint64_t>(q) * GW + gw];
-      if (!a) continue;
       if ((a >> lane) & 1u) {
         if (cur < capacity) {
           indices[cur] = q;
