@@ -85,6 +85,8 @@ def parse_args():
     ap.add_argument("--serve-inflight", type=int, default=2)
     ap.add_argument("--no-graph", action="store_true", help="time ordinary calls instead of CUDA-graph replays")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default join launch shape")
+    ap.add_argument("--join-kernel", type=int, choices=[0, 1], default=None,
+                    help="force the join kernel (0: per-lane DFS, 1: warp-cooperative frontier) after any autotuning")
     ap.add_argument("--serving-only", action="store_true", help="run only the serving measurement (prints its JSON)")
     ap.add_argument("--shard", action="store_true",
                     help="N>1: split one workload's molecules over the ranks (strong scaling, global ids kept) instead of "
@@ -378,6 +380,10 @@ def run_sigmo(args, rank, world, local):
     tuning = None
     if not args.no_autotune:
         tuning = sb.autotune(queue, qg, dg, R, ff, reps=2)
+    if args.join_kernel is not None:
+        queue.set_tuning(join_kernel=args.join_kernel)
+        if tuning is not None:
+            tuning["join_kernel"] = args.join_kernel
     graph = not args.no_graph
     for _ in range(max(args.warmup, 0)):
         res = sb.match_batched(queue, qg, dg, R, ff, None, gm)
