@@ -124,7 +124,7 @@ typedef struct sigmo_tuning {
   uint32_t join_blocks_per_sm;   /* persistent join CTAs per SM, 1..3 (3)                      */
   uint32_t join_chunk;           /* GMCR slots a lane takes per work grab, 1..64 (4)             */
   uint32_t overflow_blocks;      /* CTAs of the join for queries over 16 vertices (1184)        */
-  uint32_t overflow_serial;      /* 1 (default): run those after the main join; 0: beside it      */
+  uint32_t overflow_serial;      /* 0 (default): run those beside the main join; 1: after it       */
   uint32_t mask_chunk_slots;     /* GMCR slots per level-mask pass, in 2^20 units, 1..64 (8)     */
   uint32_t overflow_split;       /* work items per pair of those queries, each taking every
                                     split-th root candidate, 1..64 (16)                          */

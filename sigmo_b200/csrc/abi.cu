@@ -17,7 +17,7 @@
 namespace sigmo_b200 {
 
 int normalize_tuning(sigmo_tuning* t) {
-  const sigmo_tuning d{3, 4, 148 * 8, 1, 8, 16, 0};
+  const sigmo_tuning d{3, 4, 148 * 8, 0, 8, 16, 0};
   if (!t->join_blocks_per_sm) t->join_blocks_per_sm = d.join_blocks_per_sm;
   if (!t->join_chunk) t->join_chunk = d.join_chunk;
   if (!t->overflow_blocks) t->overflow_blocks = d.overflow_blocks;
