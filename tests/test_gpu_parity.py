@@ -211,6 +211,26 @@ def test_frontier_join_matches_oracle(prof, ff):
     assert ref["per_pair"].max() >= (1 if ff else 12)
 
 
+@pytest.mark.parametrize("prof", DEVICE_PROFILES)
+def test_empty_batches(prof):
+    """An empty query batch, an empty data batch, or both: zero pairs and zero
+    matches in the batched form (ordinary and graph replay) and the plain
+    stage sequence."""
+    empty = sb.io.parse("")
+    d = sb.generate_molecules(300, 10, 30, seed=5)
+    q = sb.generate_queries(10, 3, 10, seed=6)
+    for qh, dh in ((empty, d), (q, empty), (empty, empty)):
+        queue = sb.Queue(0, profile=prof)
+        qg, dg = sb.createDeviceCSRGraph(queue, qh), sb.createDeviceCSRGraph(queue, dh)
+        gm = sb.GMCR(queue)
+        for ff in (False, True):
+            for graph in (False, True, True):
+                r = sb.match_batched(queue, qg, dg, 3, ff, None, gm, graph=graph)
+                assert r["total_matches"] == 0 and r["admitted_pairs"] == 0
+        out = run_plain(qh, dh, 3, prof, False)
+        assert out["total"] == 0 and len(out["indices"]) == 0
+
+
 def test_edge_inputs():
     # a single data graph, queries of 2 vertices, a 1-vertex query, a data graph
     # with no edges, wildcard query labels and labels >= 16
