@@ -83,6 +83,7 @@ def parse_args():
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean request arrivals per second (Poisson)")
     ap.add_argument("--serve-mols", type=int, default=0, help="serving database size (0: the workload's molecules)")
     ap.add_argument("--serve-inflight", type=int, default=2)
+    ap.add_argument("--serve-batch-queries", type=int, default=64, help="most query graphs batched together")
     ap.add_argument("--no-graph", action="store_true", help="time ordinary calls instead of CUDA-graph replays")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default join launch shape")
     ap.add_argument("--join-kernel", type=int, choices=[0, 1], default=None,
@@ -294,7 +295,7 @@ def run_serving(args, d, wl, local):
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
     t_setup = time.perf_counter()
     srv = sb.Server(d, device=local, iterations=wl["R"], find_first=True, max_inflight=args.serve_inflight,
-                    max_batch_queries=64)
+                    max_batch_queries=args.serve_batch_queries)
     setup_s = time.perf_counter() - t_setup
     # warm-up: requests before the timed arrivals, some at once so that every
     # worker has run (and the memory pool holds) concurrent batches
@@ -330,7 +331,7 @@ def run_serving(args, d, wl, local):
         "database": {"molecules": d.num_graphs, "vertices": d.total_nodes, "directed_edges": d.total_edges,
                      "resident_bytes": st1["resident_bytes"], "setup_s": round(setup_s, 2)},
         "requests": n_req, "arrival_rate_per_s": args.serve_rate, "queries_per_request": "uniform 1-64",
-        "mode": "find-first", "max_inflight": args.serve_inflight, "max_batch_queries": 64,
+        "mode": "find-first", "max_inflight": args.serve_inflight, "max_batch_queries": args.serve_batch_queries,
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p95": round(float(np.percentile(lat, 95)), 3),
                        "p99": round(float(np.percentile(lat, 99)), 3), "max": round(float(lat.max()), 3)},
         "latency_ms_full_batches_p99": round(float(np.percentile(big, 99)), 3) if big else None,
