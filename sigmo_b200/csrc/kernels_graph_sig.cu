@@ -300,12 +300,19 @@ __global__ void k_graph_symmetric(uint32_t G, const uint32_t* __restrict__ goff,
                                   uint8_t* __restrict__ sym) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
     const uint32_t off = goff[g], n = goff[g + 1] - off;
+    // mirrored iff every edge u -> t (t < n) has t -> u: a missing reverse
+    // edge is found from the row that holds the edge, so only set bits are visited
     bool ok = n <= 64u * AW;
     for (uint32_t u = 0; u < n && ok; ++u)
-      for (uint32_t t = 0; t < n && ok; ++t) {
-        const bool a = (adj[static_cast<uint64_t>(off + u) * AW + (t >> 6)] >> (t & 63u)) & 1ull;
-        const bool b = (adj[static_cast<uint64_t>(off + t) * AW + (u >> 6)] >> (u & 63u)) & 1ull;
-        ok = a == b;
+      for (uint32_t w = 0; w < static_cast<uint32_t>(AW) && ok; ++w) {
+        const uint32_t lo = 64u * w;
+        uint64_t bits = lo < n ? adj[static_cast<uint64_t>(off + u) * AW + w] : 0ull;
+        if (lo < n && n - lo < 64u) bits &= (1ull << (n - lo)) - 1ull;
+        while (bits && ok) {
+          const uint32_t t = lo + static_cast<uint32_t>(__ffsll(static_cast<long long>(bits))) - 1u;
+          bits &= bits - 1;
+          ok = (adj[static_cast<uint64_t>(off + t) * AW + (u >> 6)] >> (u & 63u)) & 1ull;
+        }
       }
     sym[g] = ok ? 1 : 0;
   }
