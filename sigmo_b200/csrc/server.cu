@@ -155,7 +155,10 @@ uint64_t projected_bytes(const Graph* query, const Graph* data, bool resident) {
   const uint64_t planes = resident ? 0 : 8ull * GW * 32 * pp.K * data->adj_words;
   const uint64_t ne = 4ull * pp.C * GW + 4ull * QG * GW;
   const uint64_t gmcr = 4ull * (G + 1) + pairs * (4 + 4 + 8);
-  const uint64_t join = std::min<uint64_t>(pairs, 8ull << 20) * (8ull * 16 + 16) + 4ull * pairs;
+  // level masks + setup records per chunk of slots (two chunk buffers, one per
+  // stream, once the pairs exceed one chunk), and the overflow list
+  const uint64_t chunk = std::min<uint64_t>(pairs, 8ull << 20);
+  const uint64_t join = (pairs > chunk ? 2 : 1) * chunk * (8ull * 16 + 16) + 4ull * pairs;
   const uint64_t results = pairs * (4 + 4 + 4 + 8);
   return planes + ne + gmcr + join + results + (16ull << 20);
 }
