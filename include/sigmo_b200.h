@@ -118,7 +118,7 @@ SIGMO_API void sigmo_default_options(sigmo_options* o);
 
 /* Launch shape of the batched join (no reference counterpart; the
  * reference's only knob is the join work-group size above).  Zero fields take
- * the defaults (overflow_serial: 0 is a value, run beside).  sigmo_autotune
+ * the defaults (overflow_serial and join_kernel: 0 is a value).  sigmo_autotune
  * searches these on a caller's own workload. */
 typedef struct sigmo_tuning {
   uint32_t join_blocks_per_sm;   /* persistent join CTAs per SM, 1..3 (3)                      */
