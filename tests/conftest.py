@@ -20,3 +20,15 @@ def pytest_configure(config):
 @pytest.fixture(scope="session")
 def golden_dir():
     return TESTS / "golden"
+
+
+@pytest.fixture(scope="session", autouse=True)
+def _product_library_built():
+    """Builds libsigmo_b200.so (nvcc, sm_100a) when a fresh checkout lacks it;
+    the oracle's library builds itself on first use."""
+    from sigmo_b200 import _lib
+
+    if not _lib.LIB_PATH.exists():
+        from sigmo_b200 import build
+
+        build.build()
