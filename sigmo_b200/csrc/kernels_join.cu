@@ -1152,7 +1152,8 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
   const uint32_t skip = exact ? 0u : data->low_offset_graphs;
   void* buf = nullptr;
   SIGMO_TRY(dev_alloc(q, &buf, 256 + 4ull * m->total));
-  auto* ctr = static_cast<unsigned long long*>(buf);  // [0] tile cursor, [1] generic cursor, [2] overflow length
+  // [0] work cursor of the even chunks, [1] generic-join cursor, [2] overflow length, [3] odd chunks' cursor
+  auto* ctr = static_cast<unsigned long long*>(buf);
   uint32_t* overflow = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + 256);
   SIGMO_CUDA_TRY(cudaMemsetAsync(ctr, 0, 256, q->stream));
   auto* tot = reinterpret_cast<unsigned long long*>(d_total);
