@@ -76,7 +76,11 @@ def parse_args():
     ap.add_argument("--profile", choices=["ref-ptx", "exact"], default="ref-ptx")
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-sample", type=int, default=10_000, help="molecules in the CPU-baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=30_000,
+                    help="molecules in the CPU-baseline sample (also the GPU/oracle parity sample)")
+    ap.add_argument("--ref-step-mols", type=int, default=0,
+                    help="reference arm: molecules per step (0: the workload split over warm-up + timed steps, "
+                         "1,000-10,000 per step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mols", type=int, default=0, help="override the workload's molecule count (profiling runs)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the serving run (0: skip it)")
@@ -147,7 +151,9 @@ def use_all_host_threads():
 
 def cpu_baseline(q, d, wl, sample_mols, find_first, profile):
     """The oracle (CPU restatement of the reference) on the first
-    `sample_mols` molecules x all queries, every host thread."""
+    `sample_mols` molecules x all queries, every host thread.  The first
+    molecules keep their global vertex ids, so the oracle's GMCR and per-pair
+    counts for them are the full batch's (returned for the parity check)."""
     import oracle
 
     use_all_host_threads()
@@ -166,7 +172,47 @@ def cpu_baseline(q, d, wl, sample_mols, find_first, profile):
                   f"({'find-first' if find_first else 'find-all'}, {wl['R']} iterations), {dt:.2f} s",
         "matches": int(out["total"]),
         "seconds": dt,
-    }
+    }, out, ds.num_graphs
+
+
+def parity_sample(ref, n_graphs, offsets, indices, counts):
+    """The GPU's GMCR and per-pair counts of the first n_graphs molecules
+    against the oracle's for the same molecules (bit-exact comparison)."""
+    n_slots = int(offsets[n_graphs])
+    same = (np.array_equal(np.asarray(offsets[: n_graphs + 1], dtype=np.int64), ref["offsets"].astype(np.int64))
+            and np.array_equal(np.asarray(indices[:n_slots]), ref["indices"])
+            and np.array_equal(np.asarray(counts[:n_slots]), ref["per_pair"]))
+    return {"molecules": n_graphs, "admitted_pairs": n_slots, "matches": int(ref["total"]),
+            "compared": "GMCR offsets and indices, per-pair uint64 counts", "identical": bool(same)}
+
+
+def out_of_domain(q, d, offsets=None, indices=None):
+    """Pairs outside the reference's defined domain: queries of >= 30 vertices
+    (its DFS stack holds 30 frames, isomorphism.hpp:288,322) and molecules of
+    > 64 atoms (its 64-bit BFS / visited sets, utils.hpp:71-73,
+    signature.hpp:353-385).  The oracle defines their results."""
+    qs = np.diff(np.asarray(q.graph_offsets, dtype=np.int64))
+    ds = np.diff(np.asarray(d.graph_offsets, dtype=np.int64))
+    bq, bd = qs >= 30, ds > 64
+    nq, nd = int(bq.sum()), int(bd.sum())
+    out = {"queries_30_plus": nq, "molecules_over_64": nd,
+           "pairs": nq * len(ds) + nd * len(qs) - nq * nd,
+           "semantics": "defined by the oracle (dynamic DFS depth; BFS and visited sets over local ids < 64 under ref-ptx)"}
+    if offsets is not None:
+        g = np.repeat(np.arange(len(ds)), np.diff(np.asarray(offsets, dtype=np.int64)))
+        out["admitted_pairs"] = int((bq[np.asarray(indices, dtype=np.int64)] | bd[g]).sum())
+    return out
+
+
+def workload_config(args, wl, q, d, world, shard):
+    """The config object of the JSON line; both arms print the same one."""
+    R = wl["R"]
+    return {"workload": args.workload + ": " + wl["desc"], "molecules": d.num_graphs, "queries": q.num_graphs,
+            "data_vertices": d.total_nodes, "query_vertices": q.total_nodes, "iterations": R, "mode": args.mode,
+            "profile": args.profile, "pairs_per_step_per_gpu": q.num_graphs * d.num_graphs,
+            "l2": "inputs larger than L2: every step writes and re-reads %.0f MB of data-graph signatures "
+                  "(iterations 1..%d) plus the candidate planes" % (8 * R * d.total_nodes / 1e6, R),
+            "parallelism": (f"shards{world}" if shard else f"replicas{world}") if world > 1 else "single"}
 
 
 # ---- clocks --------------------------------------------------------------------------
@@ -442,6 +488,9 @@ def run_sigmo(args, rank, world, local):
             "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": traffic_for("join", args.workload),
             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured" else peak_kind,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the join kernels on a 20,000-molecule "
+                              "slice of this workload, scaled to this batch by admitted pairs (profiles/traffic.json); "
+                              "the join counters below come from the same capture",
             "algorithmic_bytes_per_launch": jb, "ms_per_launch": round(join_ms, 4),
             "warp_execution_efficiency": traffic_for("join", args.workload, "warp_execution_efficiency"),
             "active_warps_of_peak": traffic_for("join", args.workload, "active_warps_of_peak"),
@@ -572,9 +621,12 @@ def run_sigmo(args, rank, world, local):
     if args.serve_seconds > 0 and world == 1:
         serving = run_serving(args, d, wl, local)
 
-    cpu = None
+    cpu = parity = None
+    ood = out_of_domain(q, d, offsets, indices) if not shard else out_of_domain(q, d)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(q, d, wl, args.cpu_sample, ff, args.profile)
+        cpu, cref, n_sample = cpu_baseline(q, d, wl, args.cpu_sample, ff, args.profile)
+        parity = parity_sample(cref, n_sample, offsets, indices, gm.getPairCounts())
+        del cref
 
     if dist:
         torch.cuda.synchronize()
@@ -595,17 +647,18 @@ def run_sigmo(args, rank, world, local):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded generator; SIGMo's SMARTS/ZINC sets are not available)",
-        "config": {"workload": args.workload + ": " + wl["desc"], "molecules": d.num_graphs, "queries": q.num_graphs,
-                   "data_vertices": d.total_nodes, "query_vertices": q.total_nodes, "iterations": R, "mode": args.mode,
-                   "profile": args.profile, "pairs_per_step_per_gpu": pairs,
-                   "l2": "inputs larger than L2: every step writes and re-reads %.0f MB of data-graph signatures "
-                         "(iterations 1..%d) plus the candidate planes" % (8 * R * dg.total_nodes / 1e6, R),
-                   "parallelism": (f"shards{world}" if shard else f"replicas{world}") if world > 1 else "single"},
+        "config": workload_config(args, wl, q, d, world, shard),
+        "value_scope": "value times CUDA-graph replays of the batched form with both graph batches resident; the query "
+                       "batch's plane program (its signatures and the host-side class program) is built once per query "
+                       "batch and cached on the query handle, so replays skip it; e2e creates both graphs every step "
+                       "and so rebuilds it",
         "latency_ms": {"p50": round(float(np.percentile(step_ms, 50)), 3), "p99": round(float(np.percentile(step_ms, 99)), 3)},
         "stages_ms": stages,
         "admitted_pairs": admitted,
         "total_matches": total_matches,
         "roofline": roof,
+        "parity_sample": parity,
+        "out_of_domain": ood,
         "plain_form": plain,
         "e2e": e2e,
         "cpu_baseline": cpu,
@@ -620,27 +673,55 @@ def run_sigmo(args, rank, world, local):
 
 # ---- the reference arm ------------------------------------------------------------------
 def run_reference(args, rank, world, local):
+    """The reference's algorithm on the host cores: the oracle (its CPU
+    restatement; the SYCL reference cannot be compiled here) on the same
+    workload and config as the sigmo arm.  Inputs come from the host-only
+    workload library (oracle/libsigmo_workload.so, the same seeded
+    generator), so this arm never maps the product's CUDA library.  Each step
+    runs the full pipeline on the next contiguous slice of the workload's
+    molecules (ids re-based to 0) x all queries, so the warm-up and timed
+    steps together walk the whole workload."""
     if rank != 0:
         return
     import oracle
+    from oracle import workload
 
     wl = WORKLOADS[args.workload]
     ff = args.mode == "find-first"
-    q, d = make_workload(wl, 0)
+    d = workload.generate_molecules(wl["mols"], wl["min_atoms"], wl["max_atoms"], seed=wl["seed_d"], kind=wl["kind"],
+                                    median=wl["median"])
+    q = workload.generate_queries(wl["queries"], wl["qmin"], wl["qmax"], seed=wl["seed_q"], kind=wl["qkind"],
+                                  skew_lo=wl["skew"][0], skew_hi=wl["skew"][1])
     prof = {"ref-ptx": oracle.REF_PTX, "exact": oracle.EXACT}[args.profile]
-    sample = min(args.cpu_sample // 5 if args.cpu_sample >= 5 else 1, d.num_graphs) or 1
-    ds = d.slice(0, sample)
-    pairs = q.num_graphs * ds.num_graphs
+    total_steps = max(args.warmup, 0) + max(args.steps, 1)
+    per_step = args.ref_step_mols or min(10_000, max(1_000, -(-d.num_graphs // total_steps)))
+    per_step = max(1, min(per_step, d.num_graphs))
     use_all_host_threads()
-    for _ in range(max(args.warmup, 0)):
-        oracle.run_pipeline(q, ds, wl["R"], prof, ff)
-    times = []
-    for _ in range(args.steps):
+    cursor = 0
+
+    def step():
+        nonlocal cursor
+        if cursor >= d.num_graphs:
+            cursor = 0
+        ds = workload.slice_graphs(d, cursor, per_step)
+        cursor += ds.num_graphs
         t0 = time.perf_counter()
         out = oracle.run_pipeline(q, ds, wl["R"], prof, ff)
-        times.append(time.perf_counter() - t0)
-    dt = sum(times) / len(times)
-    v = pairs / dt
+        return time.perf_counter() - t0, q.num_graphs * ds.num_graphs, int(out["total"])
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    times, pairs, matches = [], 0, 0
+    for _ in range(args.steps):
+        dt, p, m = step()
+        times.append(dt)
+        pairs += p
+        matches += m
+    v = pairs / sum(times)
+    sample = (f"{args.steps} timed steps, each the full pipeline on the next {per_step} molecules of the workload (ids "
+              f"re-based to 0) x all {q.num_graphs} queries ({'find-first' if ff else 'find-all'}, {wl['R']} "
+              f"iterations); the SYCL reference cannot be compiled here (no SYCL compiler), so its CPU restatement "
+              f"runs on all host threads")
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -649,22 +730,19 @@ def run_reference(args, rank, world, local):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(dt * 1e3, 3),
+        "ms_per_step": round(sum(times) / len(times) * 1e3, 3),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "u32",
-        "data": "synthetic (seeded generator)",
-        "config": {"workload": args.workload + ": " + wl["desc"], "mode": args.mode, "profile": args.profile,
-                   "step_sample": f"first {ds.num_graphs} molecules x {q.num_graphs} queries per step"},
+        "data": "synthetic (seeded generator; SIGMo's SMARTS/ZINC sets are not available)",
+        "config": workload_config(args, wl, q, d, 1, False),
         "latency_ms": {"p50": round(float(np.percentile(times, 50)) * 1e3, 3),
                        "p99": round(float(np.percentile(times, 99)) * 1e3, 3)},
         "cpu_baseline": {"value": round(v, 1), "unit": "pairs/s", "cores": int(oracle.lib().orc_num_threads()),
-                         "kind": "port",
-                         "sample": f"first {ds.num_graphs} molecules x {q.num_graphs} queries, full pipeline; the SYCL "
-                                   f"reference cannot be compiled here (no SYCL compiler), so its CPU restatement runs"},
+                         "kind": "port", "sample": sample},
         "e2e": {"value": round(v, 1), "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "total_matches_sample": int(out["total"]),
+        "total_matches_timed_steps": matches,
     }
     print(json.dumps(line))
 

@@ -141,6 +141,17 @@ SIGMO_API int sigmo_queue_stream(sigmo_queue_t q, void** stream);
 /* The join launch shape used by this queue (defaults until set). */
 SIGMO_API int sigmo_queue_set_tuning(sigmo_queue_t q, const sigmo_tuning* t);
 SIGMO_API int sigmo_queue_get_tuning(sigmo_queue_t q, sigmo_tuning* t);
+/* Step budget of the join kernels (no reference counterpart: the reference's
+ * DFS, isomorphism.hpp:330-371, runs until it is done).  steps = the most DFS
+ * levels one lane may leave (backtrack from) in one launch, counted per
+ * thread of the per-lane joins and per warp of the warp-cooperative one; 0
+ * (default) = no limit.  A lane that uses its budget up stops, raises a status
+ * word, and lanes that see the word take no further pairs; the call then
+ * returns SIGMO_ERR_TIMEOUT and its counts are incomplete.  For callers that
+ * must bound the device time of a request (a serving loop that fails one
+ * pathological batch instead of holding the GPU). */
+SIGMO_API int sigmo_queue_set_join_budget(sigmo_queue_t q, uint64_t steps);
+SIGMO_API int sigmo_queue_get_join_budget(sigmo_queue_t q, uint64_t* steps);
 /* BatchedEvent::getProfilingInfo (library/include/utils.hpp:149-157): device
  * time of the last stage launched on the queue, after it has completed. */
 SIGMO_API int sigmo_queue_last_stage_ms(sigmo_queue_t q, double* ms);
@@ -262,13 +273,15 @@ SIGMO_API int sigmo_gmcr_download(sigmo_gmcr_t m, uint32_t* offsets, uint64_t of
  * exceeds capacity).  Intermediates live in one 32 MiB device array that is
  * part of the library (every GPU that loads it holds the array until exit):
  * batches needing more (query vertices x ceil(data graphs / 32) x 4 bytes plus
- * query graphs x the same, plus 4 bytes per data graph) are rejected with
+ * query graphs x the same, plus 4 bytes per data graph, plus the device scan's
+ * temporary storage, each piece rounded up to 256 bytes) are rejected with
  * SIGMO_ERR_DOMAIN.  The first call on a device resolves the array's device
  * address; make that first call before any stream capture.  Every call shares
  * the array, so calls whose work overlaps on the GPU (several queues or
- * threads at once) race; the array keeps the last call's contents.  The call
- * synchronises its queue once (to read the total); its last kernel may still
- * be running on return — wait on the queue before reading d_indices. */
+ * threads at once) race; the array keeps the last call's contents.  Every
+ * call, not only the first, waits on its queue once (cudaStreamSynchronize,
+ * to read the admitted total back to the host); its last kernel may still be
+ * running on return — wait on the queue before reading d_indices. */
 SIGMO_API int sigmo_gmcr_generate_noalloc(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c,
                                           uint32_t* d_offsets, uint32_t* d_indices, uint64_t capacity, uint64_t* total);
 
@@ -354,6 +367,9 @@ typedef struct sigmo_server_options {
   uint64_t memory_budget;      /* device bytes the running batches may hold (0: half the free memory
                                   after the database is resident)                              */
   uint32_t batch_window_us;    /* wait up to this long for a batch to fill (default 0)        */
+  uint64_t join_step_budget;   /* the workers' join step budget (sigmo_queue_set_join_budget;
+                                  0, the default: none); a batch that runs out fails its
+                                  requests with SIGMO_ERR_TIMEOUT and the server goes on      */
 } sigmo_server_options;
 
 enum { SIGMO_REQUEST_PAIRS = 1 };  /* keep the matched (query, molecule, count) list */

@@ -71,6 +71,8 @@ def lib():
         L.orc_sig_get.restype = u32
         L.orc_sig_increment.argtypes = [u64, u32, u32]
         L.orc_sig_increment.restype = u64
+        L.orc_digest.argtypes = [vp, u64, u64]
+        L.orc_digest.restype = u64
         L.orc_num_threads.restype = i32
         L.orc_set_num_threads.argtypes = [i32]
         _lib = L
@@ -278,29 +280,34 @@ def join_wildcard(qg, dg, bits, offsets, indices, profile: int = REF_PTX, find_f
     return int(total), per[: int(offsets[-1])]
 
 def run_pipeline(qg, dg, iterations: int, profile: int = REF_PTX, find_first: bool = False, wg: int = 128,
-                 keep: bool = False, skip_join: bool = False):
+                 keep: bool = False, skip_join: bool = False, digests: bool = False):
     """The driver's stage order (library/src/sigmo.cpp:98-160): data then query
     signatures, label filter, R x (refine data sigs, refine query sigs, refine
     candidates), GMCR, join.  keep=True records signatures / bitsets of every
-    iteration."""
+    iteration; digests=True records only the bitset digest after the filter
+    and after every refinement (out["digests"], R + 1 values) — the form for
+    full-size batches whose bitsets take gigabytes."""
     q, d = as_batch(qg), as_batch(dg)
     sd = generate_signatures(d)
     sq = generate_signatures(q)
     bits = filter_candidates(q, d)
-    out = {"bitsets": [], "sig_data": [], "sig_query": []}
-    if keep:
-        out["bitsets"].append(bits.copy())
-        out["sig_data"].append(sd.copy())
-        out["sig_query"].append(sq.copy())
+    out = {"bitsets": [], "sig_data": [], "sig_query": [], "digests": []}
+
+    def record():
+        if keep:
+            out["bitsets"].append(bits.copy())
+            out["sig_data"].append(sd.copy())
+            out["sig_query"].append(sq.copy())
+        if digests:
+            out["digests"].append(digest_fast(bits))
+
+    record()
     rd, rq = new_reach(d.total_nodes, profile), new_reach(q.total_nodes, profile)
     for r in range(1, iterations + 1):
         refine_signatures(d, r, profile, sd, rd)
         refine_signatures(q, r, profile, sq, rq)
         refine_candidates(q, d, sq, sd, bits)
-        if keep:
-            out["bitsets"].append(bits.copy())
-            out["sig_data"].append(sd.copy())
-            out["sig_query"].append(sq.copy())
+        record()
     out["bits"] = bits
     if skip_join:
         return out
@@ -331,3 +338,11 @@ def digest(bits: np.ndarray) -> int:
         h = _mix64(bits.astype(np.uint64) ^ w[None, :]).sum(axis=1, dtype=np.uint64)
         qv = np.arange(bits.shape[0], dtype=np.uint64) * K2
         return int(_mix64(h + qv).sum(dtype=np.uint64))
+
+
+def digest_fast(bits: np.ndarray) -> int:
+    """digest() computed by the oracle library (OpenMP), for large bitsets."""
+    if bits.size == 0:
+        return 0
+    b = np.ascontiguousarray(bits, dtype=np.uint32)
+    return int(lib().orc_digest(_ptr(b), b.shape[0], b.shape[1]))

@@ -705,6 +705,30 @@ uint64_t orc_sig_set(uint64_t s, uint32_t label, uint32_t count) { return sig_se
 uint32_t orc_sig_get(uint64_t s, uint32_t label) { return sig_get(s, label); }
 uint64_t orc_sig_increment(uint64_t s, uint32_t label, uint32_t add) { return sig_increment(s, label, add); }
 
+// Order-independent digest of a dense [rows][W] candidate bitset, the value
+// the library's sigmo_candidates_digest returns for the same bits:
+//   sum_q mix64(h_q + q*K2),  h_q = sum_w mix64(word ^ (w*K1))  (mod 2^64).
+// Not a reference function: it lets full-size bitsets (gigabytes) be compared
+// after every refinement iteration without keeping or moving them.
+static inline uint64_t digest_mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+uint64_t orc_digest(const uint32_t* bits, uint64_t rows, uint64_t W) {
+  const uint64_t K1 = 0x9E3779B97F4A7C15ull, K2 = 0xC2B2AE3D27D4EB4Full;
+  uint64_t total = 0;
+#pragma omp parallel for schedule(static) reduction(+ : total)
+  for (int64_t r = 0; r < static_cast<int64_t>(rows); ++r) {
+    const uint32_t* row = bits + static_cast<uint64_t>(r) * W;
+    uint64_t h = 0;
+    for (uint64_t w = 0; w < W; ++w) h += digest_mix64(static_cast<uint64_t>(row[w]) ^ (w * K1));
+    total += digest_mix64(h + static_cast<uint64_t>(r) * K2);
+  }
+  return total;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -249,6 +249,17 @@ class Queue:
         check(lib().sigmo_queue_get_tuning(self._h, ctypes.byref(t)))
         return {f: getattr(t, f) for f, _ in _L.TuningC._fields_}
 
+    def set_join_budget(self, steps: int):
+        """Step budget of the join kernels (sigmo_queue_set_join_budget): the
+        most DFS levels one lane may leave per launch, 0 for no limit; a join
+        that runs out raises SigmoError with code SIGMO_ERR_TIMEOUT (7)."""
+        check(lib().sigmo_queue_set_join_budget(self._h, int(steps)))
+
+    def join_budget(self) -> int:
+        v = ctypes.c_uint64()
+        check(lib().sigmo_queue_get_join_budget(self._h, ctypes.byref(v)))
+        return v.value
+
     def launch_count(self) -> int:
         v = ctypes.c_uint64()
         check(lib().sigmo_queue_launch_count(self._h, ctypes.byref(v)))
@@ -612,7 +623,7 @@ class Server:
 
     def __init__(self, database: HostGraphs, device: int = 0, profile="ref-ptx", iterations: int = 6,
                  find_first: bool = True, max_inflight: int = 2, max_batch_queries: int = 64, memory_budget: int = 0,
-                 batch_window_us: int = 0, join_work_group_size: int = 128):
+                 batch_window_us: int = 0, join_work_group_size: int = 128, join_step_budget: int = 0):
         if isinstance(profile, str):
             profile = PROFILE_NAMES[profile]
         opts = _L.OptionsC(int(profile), join_work_group_size, 512)
@@ -620,6 +631,7 @@ class Server:
         lib().sigmo_server_default_options(ctypes.byref(so))
         so.iterations, so.find_first, so.max_inflight = iterations, int(bool(find_first)), max_inflight
         so.max_batch_queries, so.memory_budget, so.batch_window_us = max_batch_queries, memory_budget, batch_window_us
+        so.join_step_budget = join_step_budget
         h = ctypes.c_void_p()
         check(lib().sigmo_server_create(device, ctypes.byref(database._raw), ctypes.byref(opts), ctypes.byref(so),
                                         ctypes.byref(h)))

@@ -64,6 +64,7 @@ class ServerOptionsC(ctypes.Structure):
         ("max_batch_queries", ctypes.c_uint32),
         ("memory_budget", ctypes.c_uint64),
         ("batch_window_us", ctypes.c_uint32),
+        ("join_step_budget", ctypes.c_uint64),
     ]
 
 
@@ -162,6 +163,8 @@ SIGNATURES = {
     "sigmo_match_batched": (_i, [_vp, _vp, _vp, _u32, _i, _u32, _vp, _vp, _P(MatchResultC)]),
     "sigmo_queue_set_tuning": (_i, [_vp, _P(TuningC)]),
     "sigmo_queue_get_tuning": (_i, [_vp, _P(TuningC)]),
+    "sigmo_queue_set_join_budget": (_i, [_vp, ctypes.c_uint64]),
+    "sigmo_queue_get_join_budget": (_i, [_vp, _P(ctypes.c_uint64)]),
     "sigmo_autotune": (_i, [_vp, _vp, _vp, _u32, _i, _u32, _P(TuningC), _P(_d), _P(_d)]),
     "sigmo_server_default_options": (None, [_P(ServerOptionsC)]),
     "sigmo_server_create": (_i, [_i, _P(HostGraphsC), _vp, _P(ServerOptionsC), _P(_vp)]),

@@ -94,6 +94,23 @@ int queue_scratch(Queue* q, size_t bytes, void** p) {
   return SIGMO_OK;
 }
 
+int join_status_reset(Queue* q) {
+  SIGMO_CUDA_TRY(cudaMemsetAsync(q->d_status, 0, sizeof(unsigned int), q->stream));
+  return SIGMO_OK;
+}
+int join_status_fetch(Queue* q) {
+  SIGMO_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(q->pinned) + kPinnedStatusOffset, q->d_status, sizeof(unsigned int),
+                                 cudaMemcpyDeviceToHost, q->stream));
+  return SIGMO_OK;
+}
+int join_status_result(Queue* q) {
+  const unsigned st = *reinterpret_cast<const unsigned*>(static_cast<const char*>(q->pinned) + kPinnedStatusOffset);
+  if (st & kJoinStatusBudget)
+    return fail(SIGMO_ERR_TIMEOUT, "a join lane used up the step budget of %llu DFS levels; the counts are incomplete",
+                static_cast<unsigned long long>(q->join_budget));
+  return SIGMO_OK;
+}
+
 namespace {
 
 int set_device(Queue* q) {
@@ -161,6 +178,8 @@ int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out
   if (st == cudaSuccess) st = cudaEventCreate(&q->ev_start);
   if (st == cudaSuccess) st = cudaEventCreate(&q->ev_end);
   if (st == cudaSuccess) st = cudaMallocHost(&q->pinned, 4096);
+  if (st == cudaSuccess) st = cudaMalloc(reinterpret_cast<void**>(&q->d_status), 256);
+  if (st == cudaSuccess) st = cudaMemset(q->d_status, 0, 256);
   if (st == cudaSuccess) st = cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking);
   if (st == cudaSuccess) st = cudaEventCreateWithFlags(&q->ev_fork, cudaEventDisableTiming);
   if (st == cudaSuccess) st = cudaEventCreateWithFlags(&q->ev_join, cudaEventDisableTiming);
@@ -210,6 +229,7 @@ int sigmo_queue_destroy(sigmo_queue_t q) {
   if (q->ev_start) cudaEventDestroy(q->ev_start);
   if (q->ev_end) cudaEventDestroy(q->ev_end);
   if (q->pinned) cudaFreeHost(q->pinned);
+  if (q->d_status) cudaFree(q->d_status);
   delete q;
   return SIGMO_OK;
 }
@@ -262,6 +282,18 @@ int sigmo_queue_set_tuning(sigmo_queue_t q, const sigmo_tuning* t) {
 int sigmo_queue_get_tuning(sigmo_queue_t q, sigmo_tuning* t) {
   if (!q || !t) return fail(SIGMO_ERR_INVALID, "null argument");
   *t = q->tune;
+  return SIGMO_OK;
+}
+
+int sigmo_queue_set_join_budget(sigmo_queue_t q, uint64_t steps) {
+  if (!q) return fail(SIGMO_ERR_INVALID, "null queue");
+  q->join_budget = steps;
+  return SIGMO_OK;
+}
+
+int sigmo_queue_get_join_budget(sigmo_queue_t q, uint64_t* steps) {
+  if (!q || !steps) return fail(SIGMO_ERR_INVALID, "null argument");
+  *steps = q->join_budget;
   return SIGMO_OK;
 }
 
@@ -696,14 +728,17 @@ int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t da
   uint64_t* d_total = nullptr;
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
   SIGMO_CUDA_TRY(cudaMemsetAsync(d_total, 0, 8, q->stream));
-  int rc = launch_join_literal(q, query, data, c, m, find_first, 0, data->num_graphs, d_total, 0, 0xFFFFFFFFu);
+  int rc = join_status_reset(q);
+  if (!rc) rc = launch_join_literal(q, query, data, c, m, find_first, 0, data->num_graphs, d_total, 0, 0xFFFFFFFFu);
   if (!rc) rc = stage_end(q);
+  if (!rc) rc = join_status_fetch(q);
   if (!rc) {
     cudaError_t e = cudaMemcpyAsync(q->pinned, d_total, 8, cudaMemcpyDeviceToHost, q->stream);
     if (e == cudaSuccess && per_pair && m->total) e = cudaMemcpyAsync(per_pair, m->counts, 8 * m->total, cudaMemcpyDeviceToHost, q->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(q->stream);
     if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "join read-back failed: %s", cudaGetErrorString(e));
-    else {
+    else rc = join_status_result(q);
+    if (!rc) {
       *num_matches += *static_cast<uint64_t*>(q->pinned);
       m->counts_valid = true;
     }

@@ -560,6 +560,7 @@ int replay_graph(Queue* q, Graph* query, Graph* data, Gmcr* m, sigmo_match_resul
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return fail(SIGMO_ERR_CUDA, "graph replay failed: %s", cudaGetErrorString(e));
+  SIGMO_TRY(join_status_result(q));  // the graph read the status word back
   const uint64_t* pin = static_cast<const uint64_t*>(q->pinned);
   const uint32_t gtotal = *reinterpret_cast<const uint32_t*>(pin + 1);
   if (gtotal != m->total) {
@@ -585,13 +586,15 @@ int capture_graph(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   const uint64_t launches0 = q->launches;
   SIGMO_CUDA_TRY(cudaStreamBeginCapture(q->stream, cudaStreamCaptureModeThreadLocal));
   uint64_t* d_total = nullptr;
-  int rc = dev_alloc(q, reinterpret_cast<void**>(&d_total), 8);
+  int rc = join_status_reset(q);
+  if (!rc) rc = dev_alloc(q, reinterpret_cast<void**>(&d_total), 8);
   if (!rc && cudaMemsetAsync(d_total, 0, 8, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
   if (!rc) rc = batched_planes(q, query, data, R, find_first, m, d_total, ev, run);
   uint64_t* pin = static_cast<uint64_t*>(q->pinned);
   if (!rc && (cudaMemcpyAsync(pin, d_total, 8, cudaMemcpyDeviceToHost, q->stream) != cudaSuccess ||
               cudaMemcpyAsync(pin + 1, m->offsets + data->num_graphs, 4, cudaMemcpyDeviceToHost, q->stream) != cudaSuccess))
     rc = fail(SIGMO_ERR_CUDA, "capture of the read-back failed");
+  if (!rc) rc = join_status_fetch(q);
   if (d_total) dev_free(q, d_total);
   cudaGraph_t g = nullptr;
   const cudaError_t ec = cudaStreamEndCapture(q->stream, &g);
@@ -622,18 +625,20 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
                 data->max_nodes);
   SIGMO_CUDA_TRY(cudaSetDevice(q->device));
   const sigmo_tuning& tn = q->tune;
-  const uint64_t key[6] = {query->stamp, data->stamp, R, static_cast<uint64_t>(find_first),
+  const uint64_t key[7] = {query->stamp, data->stamp, R, static_cast<uint64_t>(find_first),
                            static_cast<uint64_t>(q->opts.profile) | (static_cast<uint64_t>(tn.overflow_serial) << 8) |
                                (static_cast<uint64_t>(tn.overflow_split) << 16) |
                                (static_cast<uint64_t>(tn.join_kernel) << 24),
                            (static_cast<uint64_t>(tn.join_blocks_per_sm) << 48) | (static_cast<uint64_t>(tn.join_chunk) << 40) |
-                               (static_cast<uint64_t>(tn.mask_chunk_slots) << 32) | tn.overflow_blocks};
-  if (graph && !materialize && m->graph && std::equal(key, key + 6, m->graph_key)) {
+                               (static_cast<uint64_t>(tn.mask_chunk_slots) << 32) | tn.overflow_blocks,
+                           q->join_budget};
+  if (graph && !materialize && m->graph && std::equal(key, key + 7, m->graph_key)) {
     const int rc = replay_graph(q, query, data, m, out);
     if (rc != SIGMO_ERR_INVALID) return rc;  // else: recapture below
   }
   drop_graph(m);  // this run may replace the arrays a captured batch refers to
   std::memset(out, 0, sizeof(*out));
+  SIGMO_TRY(join_status_reset(q));
   Events ev;
   for (auto& e : ev.e) SIGMO_CUDA_TRY(cudaEventCreate(&e));
   SIGMO_CUDA_TRY(cudaEventRecord(ev.e[0], q->stream));
@@ -664,11 +669,13 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
     }
   }
   if (!rc && cudaEventRecord(ev.e[4], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
+  if (!rc) rc = join_status_fetch(q);
   if (!rc) {
     cudaError_t e = cudaMemcpyAsync(q->pinned, d_total, 8, cudaMemcpyDeviceToHost, q->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(q->stream);
     if (e != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "batched read-back failed: %s", cudaGetErrorString(e));
   }
+  if (!rc) rc = join_status_result(q);
   if (!rc) {
     out->total_matches = *static_cast<uint64_t*>(q->pinned);
     out->admitted_pairs = m->total;
@@ -690,7 +697,7 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   if (!rc && graph && !bitset_route) {
     // graph mode: capture this batch for the next calls with the same inputs
     rc = capture_graph(q, query, data, R, find_first, m, run);
-    if (!rc) std::copy(key, key + 6, m->graph_key);
+    if (!rc) std::copy(key, key + 7, m->graph_key);
   }
   return rc;
 }

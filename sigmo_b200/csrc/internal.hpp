@@ -47,7 +47,31 @@ struct Queue {
   // each stream's last level-mask pass
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_aux_fork = nullptr, ev_aux_join = nullptr, ev_masks[2] = {nullptr, nullptr};
+  // Join step budget (0: none) and the device status word the join kernels
+  // raise when a lane runs out of it (kJoinStatusBudget).
+  uint64_t join_budget = 0;
+  unsigned int* d_status = nullptr;
 };
+
+// What a join kernel gets of the queue's step budget: the most DFS levels one
+// lane (one warp for the frontier join) may leave in a launch, 0 for no limit,
+// and the status word it sets when the budget runs out; the lane then stops,
+// and lanes that see the word take no further work.
+struct JoinLimit {
+  uint64_t budget;
+  unsigned int* status;
+};
+constexpr unsigned kJoinStatusBudget = 1u;
+inline JoinLimit join_limit(const Queue* q) { return JoinLimit{q->join_budget, q->d_status}; }
+// Byte offset in the queue's pinned buffer where the status word is read back.
+constexpr size_t kPinnedStatusOffset = 64;
+// Clears the status word on the queue's stream (before the join kernels).
+int join_status_reset(Queue* q);
+// Queues the read-back of the status word into the pinned buffer (before the
+// host synchronises), and after the synchronisation turns a raised word into
+// SIGMO_ERR_TIMEOUT.
+int join_status_fetch(Queue* q);
+int join_status_result(Queue* q);
 
 // A contiguous range of query graphs whose planes and classes fit one
 // k_planes_admit tile in shared memory (a batch too large for one tile is
@@ -158,7 +182,7 @@ struct Gmcr {
   bool counts_valid = false;
   // CUDA graph of the last batched match run in graph mode, and what it was built for
   cudaGraphExec_t graph = nullptr;
-  uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+  uint64_t graph_key[7] = {0, 0, 0, 0, 0, 0, 0};  // inputs, mode, profile, tuning, join budget
   uint64_t graph_launches = 0;  // kernels in the captured batch
 };
 

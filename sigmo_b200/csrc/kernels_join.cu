@@ -29,6 +29,20 @@
 namespace sigmo_b200 {
 namespace {
 
+// Step budget (JoinLimit): a lane counts the DFS levels it leaves; past the
+// budget it raises the status word and stops.  Lanes check the word before
+// taking more work, so a spent budget ends the launch soon after.
+__device__ __forceinline__ bool budget_spent(const JoinLimit& lim, uint64_t& steps) {
+  if (lim.budget && ++steps > lim.budget) {
+    atomicOr(lim.status, kJoinStatusBudget);
+    return true;
+  }
+  return false;
+}
+__device__ __forceinline__ bool join_stopped(const JoinLimit& lim) {
+  return lim.budget && *reinterpret_cast<volatile const unsigned int*>(lim.status) != 0u;
+}
+
 // getCandidatesCount(src, s, e) on one bitset row.
 __device__ __forceinline__ uint32_t cand_count(const uint32_t* __restrict__ row, uint32_t s, uint32_t e, int prof) {
   const uint32_t i0 = s >> 5, i1 = (e + 31u) >> 5;
@@ -126,9 +140,11 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
                                const uint32_t* __restrict__ droff, const uint32_t* __restrict__ dcol,
                                const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ indices, uint32_t g0,
                                uint32_t g1, uint32_t q_begin, uint32_t q_end, int find_first, uint64_t* __restrict__ counts,
-                               unsigned long long* __restrict__ d_total) {
+                               unsigned long long* __restrict__ d_total, JoinLimit lim) {
   const uint32_t wg = blockDim.x, lid = threadIdx.x;
   uint64_t my_total = 0;
+  uint64_t steps = 0;
+  bool stop = false;
   PairCands pc;
   uint64_t rowc[kMaxQueryNodes];   // adjacency row of mapping[i] (graphs <= 64 vertices)
   uint64_t vmask[kMaxQueryNodes];  // candidates passing isValidMapping at depth d (graphs <= 64 vertices)
@@ -159,6 +175,10 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
 #pragma unroll 1
     for (uint32_t k = 0; k <= kMaxQueryNodes; ++k) mapping[k] = 0;
     for (uint32_t it = lid; it < seglen; it += wg) {
+      if (join_stopped(lim)) {
+        stop = true;
+        break;
+      }
       const uint32_t qg = indices[seg0 + it];
       const uint32_t qoff = qgoff[qg], n = qgoff[qg + 1] - qoff;
       if (small) pc.load(bits, Wp, qoff, n, s, e, prof);
@@ -229,12 +249,20 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
             --top;
             visited &= ~refbit(mapping[qn], s);
             if (top == 1) visited = 0;
+            if (budget_spent(lim, steps)) {
+              stop = true;
+              break;
+            }
             continue;
           }
           if (fr.idx >= count_of(qn)) {
             --top;
             visited &= ~refbit(mapping[qn], s);
             if (top == 1) visited = 0;
+            if (budget_spent(lim, steps)) {
+              stop = true;
+              break;
+            }
             continue;
           }
           const uint32_t cand = cand_of(qn, fr.idx);
@@ -270,6 +298,10 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
           }
           if (fr.idx >= count_of(qn)) {
             --top;
+            if (budget_spent(lim, steps)) {
+              stop = true;
+              break;
+            }
             continue;
           }
           const uint32_t cand = cand_of(qn, fr.idx);
@@ -286,11 +318,170 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
           }
         }
       }
+      if (stop) break;
+      counts[seg0 + it] = found;
+      my_total += found;
+    }
+    if (stop) break;
+  }
+  // block reduction, one atomic per block
+  for (int o = 16; o; o >>= 1) my_total += __shfl_xor_sync(0xFFFFFFFFu, my_total, o);
+  __shared__ uint64_t part[32];
+  if ((lid & 31u) == 0) part[lid >> 5] = my_total;
+  __syncthreads();
+  if (lid < 32) {
+    uint64_t v = lid < ((wg + 31u) >> 5) ? part[lid] : 0ull;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if (lid == 0 && v) atomicAdd(d_total, static_cast<unsigned long long>(v));
+  }
+}
+
+// k_join_literal for its common case: every data graph of the launch has at
+// most 64 vertices and every query at most kLitLevels.  The same DFS, step for
+// step, with the per-level state of each thread in shared memory
+// ([level][thread], no local-memory stack):
+//   cm[j]   the pair's range-masked candidates of query vertex j as graph-local
+//           bits (candidates.hpp:86-162; at most 3 bitset words per graph);
+//   rem[j]  the candidates the frame at depth j has still to try, taken in
+//           ascending order like getCandidateAt(idx) for idx = 0, 1, ...
+//           Only those passing isValidMapping are kept (its result depends on
+//           mapping[0..j-1], fixed while the frame runs, so it is one AND
+//           when the frame is pushed); the others are skipped by the
+//           reference with no effect, so the placements are the same;
+//   row[j]  the adjacency row of mapping[j];
+//   map[j]  mapping[j] as a local id, carried across the thread's pairs of a
+//           data graph like the reference's private array (isomorphism.hpp:309);
+//           a fresh work-item's mapping[] holds global vertex 0, which is
+//           local 0 of a graph starting at vertex 0 and kLitOutside (no
+//           bit of the graph) otherwise.
+// REF_PTX keeps the reference's `visited` bookkeeping (utils.hpp:64-96,
+// isomorphism.hpp:346-369): a frame that runs out unsets only mapping[depth]
+// (perhaps stale), and the set is cleared when the DFS is back at depth 0.
+// EXACT runs the injective DFS: the pick of a frame is unset when its child
+// frame runs out.  The last query vertex is placed in one step, as in
+// k_join_literal.
+constexpr uint32_t kLitLevels = 32;
+constexpr uint8_t kLitOutside = 0xFFu;
+constexpr size_t kLitBytesPerThread = kLitLevels * (3 * sizeof(uint64_t) + 1);
+
+template <bool EXACT>
+__global__ void k_join_literal_small(const uint32_t* __restrict__ bits, uint64_t Wp, int prof,
+                                     const uint32_t* __restrict__ qgoff, const uint64_t* __restrict__ qadj,
+                                     const uint32_t* __restrict__ dgoff, const uint64_t* __restrict__ dadj, uint32_t dAW,
+                                     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ indices, uint32_t g0,
+                                     uint32_t g1, uint32_t q_begin, uint32_t q_end, int find_first,
+                                     uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total, JoinLimit lim) {
+  extern __shared__ uint64_t lit_sm[];
+  const uint32_t wg = blockDim.x, lid = threadIdx.x;
+  uint64_t* cm = lit_sm;
+  uint64_t* rem = lit_sm + kLitLevels * wg;
+  uint64_t* row = lit_sm + 2 * kLitLevels * wg;
+  uint8_t* map = reinterpret_cast<uint8_t*>(lit_sm + 3 * kLitLevels * wg);
+#define LV(arr, l) arr[(l) * wg + lid]
+  uint64_t my_total = 0, steps = 0;
+  bool stop = false;
+  for (uint32_t g = g0 + blockIdx.x; g < g1 && !stop; g += gridDim.x) {
+    const uint32_t s = dgoff[g], e = dgoff[g + 1];
+    uint32_t seg0 = offsets[g], seg1 = offsets[g + 1];
+    if (q_begin != 0 || q_end != 0xFFFFFFFFu) {  // the segment's slots with query graph in [q_begin, q_end)
+      uint32_t lo = seg0, hi = seg1;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (indices[mid] < q_begin) lo = mid + 1;
+        else hi = mid;
+      }
+      uint32_t lo2 = lo, hi2 = seg1;
+      while (lo2 < hi2) {
+        const uint32_t mid = (lo2 + hi2) >> 1;
+        if (indices[mid] < q_end) lo2 = mid + 1;
+        else hi2 = mid;
+      }
+      seg0 = lo;
+      seg1 = lo2;
+    }
+    const uint8_t map0 = s == 0 ? 0 : kLitOutside;
+#pragma unroll 1
+    for (uint32_t k = 0; k < kLitLevels; ++k) LV(map, k) = map0;  // mapping[] of a fresh work-item
+    // graph-local bits whose global id is below 256: the only ones the
+    // reference's uint8-indexed visited set can hold
+    const uint64_t low = s >= 256u ? 0ull : (256u - s >= 64u ? ~0ull : ((1ull << (256u - s)) - 1ull));
+    const uint32_t i0 = s >> 5, nw = ((e + 31u) >> 5) - i0, sh = s & 31u;
+    for (uint32_t it = lid; it < seg1 - seg0; it += wg) {
+      if (join_stopped(lim)) {
+        stop = true;
+        break;
+      }
+      const uint32_t qg = indices[seg0 + it];
+      const uint32_t qoff = qgoff[qg], n = qgoff[qg + 1] - qoff;
+      for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t* r = bits + static_cast<uint64_t>(qoff + j) * Wp;
+        uint32_t w[3];
+#pragma unroll
+        for (uint32_t k = 0; k < 3; ++k) w[k] = k < nw ? (r[i0 + k] & range_mask(i0 + k, s, e, prof)) : 0u;
+        const uint64_t lo64 = static_cast<uint64_t>(w[0]) | (static_cast<uint64_t>(w[1]) << 32);
+        LV(cm, j) = (lo64 >> sh) | (sh ? (static_cast<uint64_t>(w[2]) << (64u - sh)) : 0ull);
+      }
+      uint64_t found = 0, visited = 0;
+      uint32_t top = 1;  // frames at depths 0 .. top-1
+      LV(rem, 0) = LV(cm, 0);
+      while (top > 0) {
+        const uint32_t qn = top - 1;
+        if (qn + 1 == n) {
+          // the last query vertex in one step: the frame was just pushed
+          uint64_t place = LV(rem, qn) & ~visited;
+          if (place) {
+            if (find_first) place &= 0ull - place;
+            found += __popcll(place);
+            if (!EXACT) {
+              visited |= place & low;
+              LV(map, qn) = static_cast<uint8_t>(63 - __clzll(static_cast<long long>(place)));
+            }
+            if (find_first) break;
+          }
+        } else {
+          const uint64_t r = LV(rem, qn);
+          if (r) {
+            const uint32_t t = __ffsll(static_cast<long long>(r)) - 1;
+            LV(rem, qn) = r & (r - 1);
+            const uint64_t bit = 1ull << t;
+            if (EXACT ? (visited & bit) : (visited & bit & low)) continue;
+            // place t at depth qn and push the frame of depth qn + 1
+            LV(map, qn) = static_cast<uint8_t>(t);
+            const uint64_t rw = dadj[static_cast<uint64_t>(s + t) * dAW];
+            LV(row, qn) = rw;
+            visited |= EXACT ? bit : (bit & low);
+            const uint32_t d = qn + 1;
+            const uint64_t qcol = qadj[qoff + d];  // bit i: query vertices i and d adjacent
+            uint64_t vm = LV(cm, d);
+            for (uint32_t i = 0; i < d; ++i) {
+              const uint64_t ri = i == qn ? rw : LV(row, i);
+              vm &= ((qcol >> i) & 1ull) ? ri : ~ri;
+            }
+            LV(rem, d) = vm;
+            ++top;
+            continue;
+          }
+        }
+        // the frame at depth qn is used up
+        --top;
+        if (EXACT) {
+          if (top) visited &= ~(1ull << LV(map, top - 1));  // the parent's pick
+        } else {
+          const uint32_t mq = LV(map, qn);  // mapping[qn], perhaps stale
+          if (mq < 64u) visited &= ~((1ull << mq) & low);
+          if (top == 1) visited = 0;
+        }
+        if (budget_spent(lim, steps)) {
+          stop = true;
+          break;
+        }
+      }
+      if (stop) break;
       counts[seg0 + it] = found;
       my_total += found;
     }
   }
-  // block reduction, one atomic per block
+#undef LV
   for (int o = 16; o; o >>= 1) my_total += __shfl_xor_sync(0xFFFFFFFFu, my_total, o);
   __shared__ uint64_t part[32];
   if ((lid & 31u) == 0) part[lid >> 5] = my_total;
@@ -510,8 +701,9 @@ __global__ void __launch_bounds__(128) k_join_fast(
     const uint8_t* __restrict__ dsym, const uint32_t* __restrict__ indices, const uint32_t* __restrict__ pair_graph,
     const uint32_t* __restrict__ list, const unsigned long long* __restrict__ list_len, uint64_t total_slots,
     uint32_t skip_below, int find_first, uint32_t split, unsigned long long* __restrict__ cursor,
-    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total) {
+    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total, JoinLimit lim) {
   constexpr uint32_t kChunk = 8;
+  uint64_t steps = 0;
   // entries to walk (list or all slots); with split > 1 every entry is split
   // into `split` work items, item p taking the root candidates of rank = p mod
   // split, and the items' counts are merged into counts[] (zeroed beforehand)
@@ -551,6 +743,10 @@ __global__ void __launch_bounds__(128) k_join_fast(
       bool done = false;
       for (;;) {
         if (next >= end) {
+          if (join_stopped(lim)) {
+            done = true;
+            break;
+          }
           const unsigned am = __activemask();
           const unsigned leader = __ffs(am) - 1;
           const unsigned rank = __popc(am & ((1u << lane) - 1u));
@@ -611,6 +807,7 @@ __global__ void __launch_bounds__(128) k_join_fast(
     for (int w = 0; w < AW; ++w) empty &= cand[k][w] == 0;
     if (empty) {
       --k;
+      if (budget_spent(lim, steps)) break;
       continue;
     }
     uint32_t t = 0;
@@ -718,8 +915,9 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
     const uint64_t* __restrict__ masks, const uint4* __restrict__ rec, uint64_t slot0, uint64_t count,
     const uint64_t* __restrict__ qsel, const uint64_t* __restrict__ qsel_id, const uint64_t* __restrict__ dadj,
     uint32_t skip_below, int find_first, uint32_t kChunk, unsigned long long* __restrict__ cursor,
-    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total) {
+    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total, JoinLimit lim) {
   extern __shared__ uint64_t sm[];
+  uint64_t steps = 0;
   const unsigned tid = threadIdx.x, lane = tid & 31u;
   uint64_t* cand = sm;
   uint64_t* base = sm + kPhaseLevels * kPhaseThreads;
@@ -739,6 +937,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
   auto fetch = [&]() {
     pre = false;
     if (next >= end) {
+      if (join_stopped(lim)) return;
       const unsigned am = __activemask();
       const unsigned leader = __ffs(am) - 1;
       const unsigned rank = __popc(am & ((1u << lane) - 1u));
@@ -786,6 +985,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_join_masks(
     if (!ck) {
       --k;
       if (EXACT && k >= 0) used &= ~(1ull << AT(pk, k));
+      if (budget_spent(lim, steps)) break;
       continue;
     }
     const uint32_t t = __ffsll(static_cast<long long>(ck)) - 1;
@@ -869,8 +1069,9 @@ __global__ void __launch_bounds__(kFrontWarps * 32, 3) k_join_frontier(
     const uint64_t* __restrict__ masks, const uint4* __restrict__ rec, uint64_t slot0, uint64_t count,
     const uint64_t* __restrict__ qsel, const uint64_t* __restrict__ qsel_id, const uint64_t* __restrict__ dadj,
     uint32_t skip_below, int find_first, uint32_t kChunk, unsigned long long* __restrict__ cursor,
-    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total) {
+    uint64_t* __restrict__ counts, unsigned long long* __restrict__ d_total, JoinLimit lim) {
   extern __shared__ __align__(16) unsigned char front_raw[];
+  uint64_t rounds = 0;
   FrontWarp& w = reinterpret_cast<FrontWarp*>(front_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
   constexpr unsigned kAll = 0xFFFFFFFFu;
@@ -884,12 +1085,21 @@ __global__ void __launch_bounds__(kFrontWarps * 32, 3) k_join_frontier(
   uint64_t my_total = 0;
   uint32_t L = 0;
   for (;;) {
+    // the budget counts this warp's rounds (warp-uniform)
+    if (lim.budget && ++rounds > lim.budget) {
+      if (lane == 0) atomicOr(lim.status, kJoinStatusBudget);
+      break;
+    }
     if (L == 0 && more) {
       // fill the free pair slots (lane i owns slot i) from the work range
       bool fr = w.pinfo[lane].z == kFrontFree;
       unsigned F = __ballot_sync(kAll, fr);
       while (F && more) {
         if (next >= end) {
+          if (__shfl_sync(kAll, join_stopped(lim) ? 1u : 0u, 0)) {
+            more = false;
+            break;
+          }
           unsigned long long b = 0;
           if (lane == 0) b = atomicAdd(cursor, 32ull * kChunk);
           b = __shfl_sync(kAll, b, 0);
@@ -1068,16 +1278,33 @@ int launch_join_literal(Queue* q, const Graph* query, const Graph* data, const C
   if (wg > 1024u || (wg & 31u)) return fail(SIGMO_ERR_INVALID, "join work-group size %u must be a multiple of 32 <= 1024", wg);
   const unsigned grid = std::min<uint32_t>(graph_end - graph_begin, 148u * 64u);
   auto* tot = reinterpret_cast<unsigned long long*>(d_total);
+  // the common case (graphs of <= 64 vertices, queries of <= kLitLevels) keeps
+  // its per-level state in shared memory
+  uint32_t range_max = data->max_nodes;
+  if (range_max > 64u) {
+    range_max = 0;
+    for (uint32_t g = graph_begin; g < graph_end; ++g)
+      range_max = std::max(range_max, data->host_graph_offsets[g + 1] - data->host_graph_offsets[g]);
+  }
+  if (range_max <= 64u && query->max_nodes <= kLitLevels && wg <= 256u) {
+    const size_t smem = kLitBytesPerThread * wg;
+    auto kern = exact ? k_join_literal_small<true> : k_join_literal_small<false>;
+    SIGMO_TRY(allow_max_dynamic_smem(reinterpret_cast<const void*>(kern), q->device));
+    kern<<<grid, wg, smem, q->stream>>>(c->bits, c->Wp, q->opts.profile, query->graph_offsets, query->adj,
+                                        data->graph_offsets, data->adj, data->adj_words, m->offsets, m->indices, graph_begin,
+                                        graph_end, q_begin, q_end, find_first, m->counts, tot, join_limit(q));
+    return check_launch(q, "k_join_literal_small");
+  }
   if (exact)
     k_join_literal<true><<<grid, wg, 0, q->stream>>>(c->bits, c->Wp, q->opts.profile, query->graph_offsets, query->adj,
                                                       data->graph_offsets, data->adj, data->adj_words, data->row_offsets,
                                                       data->column_indices, m->offsets, m->indices, graph_begin, graph_end,
-                                                      q_begin, q_end, find_first, m->counts, tot);
+                                                      q_begin, q_end, find_first, m->counts, tot, join_limit(q));
   else
     k_join_literal<false><<<grid, wg, 0, q->stream>>>(c->bits, c->Wp, q->opts.profile, query->graph_offsets, query->adj,
                                                        data->graph_offsets, data->adj, data->adj_words, data->row_offsets,
                                                        data->column_indices, m->offsets, m->indices, graph_begin, graph_end,
-                                                       q_begin, q_end, find_first, m->counts, tot);
+                                                       q_begin, q_end, find_first, m->counts, tot, join_limit(q));
   return check_launch(q, "k_join_literal");
 }
 
@@ -1131,7 +1358,8 @@ int launch_join_fast(Queue* q, const Graph* query, const Graph* data, const Cand
                                                        q->opts.profile, query->graph_offsets, query->qorder,             \
                                                        query->qsel, query->qsel_id, query->sym, data->graph_offsets,     \
                                                        data->adj, data->sym, m->indices, m->pair_graph, nullptr, nullptr, \
-                                                       m->total, skip, find_first, 1u, cursor, m->counts, tot)
+                                                       m->total, skip, find_first, 1u, cursor, m->counts, tot, \
+                                                       join_limit(q))
   switch (data->adj_words) {
     case 1: if (exact) SIGMO_JOIN_FAST(1, true); else SIGMO_JOIN_FAST(1, false); break;
     case 2: if (exact) SIGMO_JOIN_FAST(2, true); else SIGMO_JOIN_FAST(2, false); break;
@@ -1183,7 +1411,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
                                  : static_cast<size_t>(kPhaseLevels) * kPhaseThreads * (2 * 8 + 1);
     const unsigned block = frontier ? kFrontWarps * 32u : kPhaseThreads;
     void (*join_kernel)(const uint64_t*, const uint4*, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const uint64_t*,
-                        uint32_t, int, uint32_t, unsigned long long*, uint64_t*, unsigned long long*) = nullptr;
+                        uint32_t, int, uint32_t, unsigned long long*, uint64_t*, unsigned long long*, JoinLimit) = nullptr;
     switch (data->adj_words) {
       case 1:
         join_kernel = frontier ? (exact ? k_join_frontier<true, 1> : k_join_frontier<false, 1>)
@@ -1220,7 +1448,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
         const unsigned full = static_cast<unsigned>(sms) * tn.join_blocks_per_sm;
         const unsigned grid = full > reserve + static_cast<unsigned>(sms) ? full - reserve : full;
         join_kernel<<<grid, block, smem, st>>>(masks, recs, slot0, cnt, query->qsel, query->qsel_id, data->adj, skip,
-                                               find_first, tn.join_chunk, cursor, m->counts, tot);
+                                               find_first, tn.join_chunk, cursor, m->counts, tot, join_limit(q));
         rc = check_launch(q, frontier ? "k_join_frontier" : "k_join_masks");
       }
     }
@@ -1254,7 +1482,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
                                                             query->qsel, query->qsel_id, query->sym, data->graph_offsets, \
                                                             data->adj, data->sym, m->indices, m->pair_graph, list,       \
                                                             list_len, m->total, skip, find_first, split, ctr + 1, m->counts, \
-                                                            tot)
+                                                            tot, join_limit(q))
     switch (data->adj_words) {
       case 1: if (exact) SIGMO_JOIN_PLANES(1, true); else SIGMO_JOIN_PLANES(1, false); break;
       case 2: if (exact) SIGMO_JOIN_PLANES(2, true); else SIGMO_JOIN_PLANES(2, false); break;

@@ -359,6 +359,29 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
   if (e1) cudaEventDestroy(e1);
   if (qg) sigmo_graph_destroy(qg);
   const auto t_done = Clock::now();
+  // The matched pairs split into per-request lists in one pass over the
+  // batch's pairs, before the server lock is taken (requests cover contiguous
+  // query ranges of the batch, in order).
+  std::vector<std::vector<uint32_t>> req_pq(batch.size()), req_pg(batch.size());
+  std::vector<std::vector<uint64_t>> req_pc(batch.size());
+  if (!rc && !h_pq.empty()) {
+    std::vector<int32_t> owner(QG, -1);
+    std::vector<uint32_t> first_query(batch.size());
+    uint32_t qb = 0;
+    for (size_t i = 0; i < batch.size(); ++i) {
+      first_query[i] = qb;
+      if (batch[i]->flags & SIGMO_REQUEST_PAIRS)
+        for (uint32_t k = 0; k < batch[i]->num_queries; ++k) owner[qb + k] = static_cast<int32_t>(i);
+      qb += batch[i]->num_queries;
+    }
+    for (size_t p = 0; p < h_pq.size(); ++p) {
+      const int32_t i = h_pq[p] < QG ? owner[h_pq[p]] : -1;
+      if (i < 0) continue;
+      req_pq[i].push_back(h_pq[p] - first_query[i]);
+      req_pg[i].push_back(h_pg[p]);
+      req_pc[i].push_back(h_pc[p]);
+    }
+  }
   {
     std::lock_guard<std::mutex> lk(mu);
     if (reserved) {
@@ -394,12 +417,9 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
           o.total_matches += r->q_total[k];
         }
         if (r->flags & SIGMO_REQUEST_PAIRS) {
-          for (size_t p = 0; p < h_pq.size(); ++p)
-            if (h_pq[p] >= qb && h_pq[p] < qe) {
-              r->pair_q.push_back(h_pq[p] - qb);
-              r->pair_g.push_back(h_pg[p]);
-              r->pair_c.push_back(h_pc[p]);
-            }
+          r->pair_q = std::move(req_pq[i]);
+          r->pair_g = std::move(req_pg[i]);
+          r->pair_c = std::move(req_pc[i]);
         }
       }
       r->done = true;
@@ -542,6 +562,7 @@ int sigmo_server_create(int device, const sigmo_host_graphs* database, const sig
   s->workers.resize(o.max_inflight);
   for (auto& w : s->workers) {
     rc = sigmo_queue_create(device, &s->opts, &w.q);
+    if (!rc) rc = sigmo_queue_set_join_budget(w.q, o.join_step_budget);
     if (!rc) rc = sigmo_gmcr_create(w.q, &w.m);
     if (rc) break;
   }

@@ -24,11 +24,17 @@ def golden_dir():
 
 @pytest.fixture(scope="session", autouse=True)
 def _product_library_built():
-    """Builds libsigmo_b200.so (nvcc, sm_100a) when a fresh checkout lacks it;
-    the oracle's library builds itself on first use."""
-    from sigmo_b200 import _lib
+    """Brings libsigmo_b200.so (nvcc, sm_100a) up to date with its sources:
+    build.build() compares a fingerprint of csrc/, include/ and cli/ with the
+    one the last build recorded and recompiles only when they differ.  On a
+    machine without nvcc the existing library (if any) is used as it is; the
+    oracle-only tests do not need it, and a test that does reports the missing
+    library itself."""
+    from sigmo_b200 import build
 
-    if not _lib.LIB_PATH.exists():
-        from sigmo_b200 import build
-
+    try:
         build.build()
+    except RuntimeError as e:
+        import warnings
+
+        warnings.warn(f"libsigmo_b200.so not rebuilt: {e}")

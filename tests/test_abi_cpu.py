@@ -194,3 +194,19 @@ def test_local_arrays_rebuild_the_batch():
     rr.append([ebase[-1]])
     assert np.array_equal(np.concatenate(rr), g.row_offsets.astype(np.int64))
     assert np.array_equal(cols.astype(np.int64) + np.repeat(goff[:-1], e), g.column_indices.astype(np.int64))
+
+
+def test_host_workload_library_matches_the_product_generator():
+    """bench.py's reference arm makes its inputs with oracle/libsigmo_workload.so
+    (the same generator compiled for the host alone); its graphs and slices are
+    the product library's."""
+    from oracle import workload
+
+    for kind, args in ((0, (400, 10, 60)), (1, (300, 6, 120)), (2, (200, 10, 64))):
+        a = workload.generate_molecules(*args, seed=91 + kind, kind=kind)
+        b = sb.generate_molecules(*args, seed=91 + kind, kind=kind)
+        _same(b, a)
+        _same(b.slice(37, 120), workload.slice_graphs(a, 37, 120))
+    for qkind in (0, 3):
+        _same(sb.generate_queries(50, 3, 30, seed=7, kind=qkind, skew_lo=6, skew_hi=15),
+              workload.generate_queries(50, 3, 30, seed=7, kind=qkind, skew_lo=6, skew_hi=15))
