@@ -140,6 +140,50 @@ int finish_graph(Graph* g) {
 
 }  // namespace sigmo_b200
 
+namespace sigmo_b200 {
+namespace {
+
+void queue_free(Queue* q) {
+  cudaSetDevice(q->device);
+  if (q->stream) {
+    dev_free(q, q->scratch);
+    cudaStreamSynchronize(q->stream);
+    cudaStreamDestroy(q->stream);
+  }
+  if (q->side) {
+    cudaStreamSynchronize(q->side);
+    cudaStreamDestroy(q->side);
+  }
+  if (q->aux) {
+    cudaStreamSynchronize(q->aux);
+    cudaStreamDestroy(q->aux);
+  }
+  if (q->ev_fork) cudaEventDestroy(q->ev_fork);
+  if (q->ev_join) cudaEventDestroy(q->ev_join);
+  if (q->ev_aux_fork) cudaEventDestroy(q->ev_aux_fork);
+  if (q->ev_aux_join) cudaEventDestroy(q->ev_aux_join);
+  for (cudaEvent_t e : q->ev_masks)
+    if (e) cudaEventDestroy(e);
+  if (q->ev_start) cudaEventDestroy(q->ev_start);
+  if (q->ev_end) cudaEventDestroy(q->ev_end);
+  if (q->pinned) cudaFreeHost(q->pinned);
+  if (q->d_status) cudaFree(q->d_status);
+  delete static_cast<sigmo_queue_t>(q);
+}
+
+}  // namespace
+
+Queue* queue_retain(Queue* q) {
+  q->refs.fetch_add(1, std::memory_order_relaxed);
+  return q;
+}
+
+void queue_release(Queue* q) {
+  if (q->refs.fetch_sub(1, std::memory_order_acq_rel) == 1) queue_free(q);
+}
+
+}  // namespace sigmo_b200
+
 using namespace sigmo_b200;
 
 extern "C" {
@@ -206,31 +250,7 @@ int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out
 
 int sigmo_queue_destroy(sigmo_queue_t q) {
   if (!q) return SIGMO_OK;
-  cudaSetDevice(q->device);
-  if (q->stream) {
-    dev_free(q, q->scratch);
-    cudaStreamSynchronize(q->stream);
-    cudaStreamDestroy(q->stream);
-  }
-  if (q->side) {
-    cudaStreamSynchronize(q->side);
-    cudaStreamDestroy(q->side);
-  }
-  if (q->aux) {
-    cudaStreamSynchronize(q->aux);
-    cudaStreamDestroy(q->aux);
-  }
-  if (q->ev_fork) cudaEventDestroy(q->ev_fork);
-  if (q->ev_join) cudaEventDestroy(q->ev_join);
-  if (q->ev_aux_fork) cudaEventDestroy(q->ev_aux_fork);
-  if (q->ev_aux_join) cudaEventDestroy(q->ev_aux_join);
-  for (cudaEvent_t e : q->ev_masks)
-    if (e) cudaEventDestroy(e);
-  if (q->ev_start) cudaEventDestroy(q->ev_start);
-  if (q->ev_end) cudaEventDestroy(q->ev_end);
-  if (q->pinned) cudaFreeHost(q->pinned);
-  if (q->d_status) cudaFree(q->d_status);
-  delete q;
+  queue_release(q);
   return SIGMO_OK;
 }
 
@@ -314,7 +334,7 @@ int sigmo_graph_create(sigmo_queue_t q, const sigmo_host_graphs* h, sigmo_graph_
     return fail(SIGMO_ERR_INVALID, "sigmo_graph_create: offsets disagree with totals");
   sigmo_graph_t g = new (std::nothrow) sigmo_graph_s();
   if (!g) return fail(SIGMO_ERR_OOM, "host allocation failed");
-  g->q = q;
+  g->q = queue_retain(q);
   g->num_graphs = h->num_graphs;
   g->total_nodes = h->total_nodes;
   g->total_edges = h->total_edges;
@@ -352,7 +372,7 @@ int sigmo_graph_create_device(sigmo_queue_t q, uint32_t num_graphs, uint64_t tot
   SIGMO_TRY(set_device(q));
   sigmo_graph_t g = new (std::nothrow) sigmo_graph_s();
   if (!g) return fail(SIGMO_ERR_OOM, "host allocation failed");
-  g->q = q;
+  g->q = queue_retain(q);
   g->owned = false;
   g->num_graphs = num_graphs;
   g->total_nodes = total_nodes;
@@ -413,6 +433,7 @@ int sigmo_graph_destroy(sigmo_graph_t g) {
   release_plane_program(g);
   if (g->ready) cudaEventDestroy(g->ready);
   delete g;
+  queue_release(q);
   return SIGMO_OK;
 }
 
@@ -440,7 +461,7 @@ int sigmo_candidates_create(sigmo_queue_t q, uint64_t source_nodes, uint64_t tar
   SIGMO_TRY(set_device(q));
   sigmo_candidates_t c = new (std::nothrow) sigmo_candidates_s();
   if (!c) return fail(SIGMO_ERR_OOM, "host allocation failed");
-  c->q = q;
+  c->q = queue_retain(q);
   c->rows = source_nodes;
   c->targets = target_nodes;
   c->W = (target_nodes + 31) / 32;
@@ -463,8 +484,10 @@ int sigmo_candidates_create(sigmo_queue_t q, uint64_t source_nodes, uint64_t tar
 int sigmo_candidates_destroy(sigmo_candidates_t c) {
   if (!c) return SIGMO_OK;
   cudaSetDevice(c->q->device);
-  dev_free(c->q, c->bits);
+  Queue* q = c->q;
+  dev_free(q, c->bits);
   delete c;
+  queue_release(q);
   return SIGMO_OK;
 }
 
@@ -532,7 +555,7 @@ int sigmo_signature_create(sigmo_queue_t q, uint64_t data_nodes, uint64_t query_
   SIGMO_TRY(set_device(q));
   sigmo_signature_t s = new (std::nothrow) sigmo_signature_s();
   if (!s) return fail(SIGMO_ERR_OOM, "host allocation failed");
-  s->q = q;
+  s->q = queue_retain(q);
   s->data_nodes = data_nodes;
   s->query_nodes = query_nodes;
   s->reach_words = q->opts.profile == kProfileExact ? kMaxAdjWords : 1u;
@@ -564,7 +587,9 @@ int sigmo_signature_destroy(sigmo_signature_t s) {
   dev_free(s->q, s->data_reach);
   dev_free(s->q, s->query_reach);
   dev_free(s->q, s->data_planes);
+  Queue* q = s->q;
   delete s;
+  queue_release(q);
   return SIGMO_OK;
 }
 
@@ -664,7 +689,7 @@ int sigmo_gmcr_create(sigmo_queue_t q, sigmo_gmcr_t* out) {
   if (!q || !out) return fail(SIGMO_ERR_INVALID, "null argument");
   sigmo_gmcr_t m = new (std::nothrow) sigmo_gmcr_s();
   if (!m) return fail(SIGMO_ERR_OOM, "host allocation failed");
-  m->q = q;
+  m->q = queue_retain(q);
   *out = m;
   return SIGMO_OK;
 }
@@ -677,7 +702,9 @@ int sigmo_gmcr_destroy(sigmo_gmcr_t m) {
   dev_free(m->q, m->indices);
   dev_free(m->q, m->pair_graph);
   dev_free(m->q, m->counts);
+  Queue* q = m->q;
   delete m;
+  queue_release(q);
   return SIGMO_OK;
 }
 

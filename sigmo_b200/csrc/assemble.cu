@@ -96,7 +96,7 @@ extern "C" int sigmo_graph_create_from_local(sigmo_queue_t q, uint32_t num_graph
   if ((N && !node_labels) || (E && !columns_local)) return fail(SIGMO_ERR_INVALID, "sigmo_graph_create_from_local: null arrays");
   sigmo_graph_t g = new (std::nothrow) sigmo_graph_s();
   if (!g) return fail(SIGMO_ERR_OOM, "host allocation failed");
-  g->q = q;
+  g->q = queue_retain(q);
   g->num_graphs = num_graphs;
   g->total_nodes = N;
   g->total_edges = E;

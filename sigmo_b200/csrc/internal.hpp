@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <vector>
 
@@ -51,7 +52,15 @@ struct Queue {
   // raise when a lane runs out of it (kJoinStatusBudget).
   uint64_t join_budget = 0;
   unsigned int* d_status = nullptr;
+  // References: the caller's handle plus one per graph, candidate bitset,
+  // signature and GMCR created on the queue.  sigmo_queue_destroy drops the
+  // caller's; the queue (its streams, which those objects free their memory
+  // on) is released with the last reference, whatever the order of the
+  // destroy calls.
+  std::atomic<int> refs{1};
 };
+Queue* queue_retain(Queue* q);
+void queue_release(Queue* q);
 
 // What a join kernel gets of the queue's step budget: the most DFS levels one
 // lane (one warp for the frontier join) may leave in a launch, 0 for no limit,
