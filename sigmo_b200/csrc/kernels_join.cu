@@ -348,7 +348,6 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
 //           mapping[0..j-1], fixed while the frame runs, so it is one AND
 //           when the frame is pushed); the others are skipped by the
 //           reference with no effect, so the placements are the same;
-//   row[j]  the adjacency row of mapping[j];
 //   map[j]  mapping[j] as a local id, carried across the thread's pairs of a
 //           data graph like the reference's private array (isomorphism.hpp:309);
 //           a fresh work-item's mapping[] holds global vertex 0, which is
@@ -362,7 +361,9 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
 // k_join_literal.
 constexpr uint32_t kLitLevels = 32;
 constexpr uint8_t kLitOutside = 0xFFu;
-constexpr size_t kLitBytesPerThread = kLitLevels * (3 * sizeof(uint64_t) + 1);
+// 17 B per level and thread: 68 KB for the default 128 threads, so a block
+// fits beside two persistent k_join_masks CTAs on one SM.
+constexpr size_t kLitBytesPerThread = kLitLevels * (2 * sizeof(uint64_t) + 1);
 
 template <bool EXACT>
 __global__ void k_join_literal_small(const uint32_t* __restrict__ bits, uint64_t Wp, int prof,
@@ -375,8 +376,7 @@ __global__ void k_join_literal_small(const uint32_t* __restrict__ bits, uint64_t
   const uint32_t wg = blockDim.x, lid = threadIdx.x;
   uint64_t* cm = lit_sm;
   uint64_t* rem = lit_sm + kLitLevels * wg;
-  uint64_t* row = lit_sm + 2 * kLitLevels * wg;
-  uint8_t* map = reinterpret_cast<uint8_t*>(lit_sm + 3 * kLitLevels * wg);
+  uint8_t* map = reinterpret_cast<uint8_t*>(lit_sm + 2 * kLitLevels * wg);
 #define LV(arr, l) arr[(l) * wg + lid]
   uint64_t my_total = 0, steps = 0;
   bool stop = false;
@@ -447,16 +447,15 @@ __global__ void k_join_literal_small(const uint32_t* __restrict__ bits, uint64_t
             if (EXACT ? (visited & bit) : (visited & bit & low)) continue;
             // place t at depth qn and push the frame of depth qn + 1
             LV(map, qn) = static_cast<uint8_t>(t);
-            const uint64_t rw = dadj[static_cast<uint64_t>(s + t) * dAW];
-            LV(row, qn) = rw;
             visited |= EXACT ? bit : (bit & low);
+            // isValidMapping for depth d = qn + 1 against mapping[0..qn]: the
+            // data rows of the picks (graph-local adjacency words) must equal
+            // the query's adjacency to d, bit for bit
             const uint32_t d = qn + 1;
             const uint64_t qcol = qadj[qoff + d];  // bit i: query vertices i and d adjacent
-            uint64_t vm = LV(cm, d);
-            for (uint32_t i = 0; i < d; ++i) {
-              const uint64_t ri = i == qn ? rw : LV(row, i);
-              vm &= ((qcol >> i) & 1ull) ? ri : ~ri;
-            }
+            uint64_t vm = LV(cm, d) & ~(dadj[static_cast<uint64_t>(s + t) * dAW] ^ (0ull - ((qcol >> qn) & 1ull)));
+            for (uint32_t i = 0; i < qn; ++i)
+              vm &= ~(dadj[static_cast<uint64_t>(s + LV(map, i)) * dAW] ^ (0ull - ((qcol >> i) & 1ull)));
             LV(rem, d) = vm;
             ++top;
             continue;
