@@ -390,6 +390,9 @@ typedef struct sigmo_request_result {
   double ms_filter;            /* the batch's stages (CUDA events; sigmo_match_result)         */
   double ms_mapping;
   double ms_join;
+  uint64_t gathered_plane_bytes; /* resident plane rows the batch's admission read (0 when the
+                                    planes were built for the batch); / ms_filter = its
+                                    gather bandwidth                                           */
 } sigmo_request_result;
 
 typedef struct sigmo_server_stats {

@@ -85,6 +85,7 @@ class RequestResultC(ctypes.Structure):
         ("ms_filter", ctypes.c_double),
         ("ms_mapping", ctypes.c_double),
         ("ms_join", ctypes.c_double),
+        ("gathered_plane_bytes", ctypes.c_uint64),
     ]
 
 

@@ -238,6 +238,7 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
   uint64_t reserved = 0, batch_id = 0;
   sigmo_graph_t qg = nullptr;
   sigmo_match_result mr{};
+  uint64_t gathered = 0;  // resident plane bytes the admission gathered
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   float dev_ms = 0;
   std::vector<unsigned long long> h_matched(QG), h_sum(QG);
@@ -280,6 +281,8 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
     run.query_ranges = ranges.data();
     run.nranges = static_cast<uint32_t>(batch.size());
     note(match_batched(q, qg, data, so.iterations, so.find_first, false, nullptr, w->m, &mr, run));
+    if (!rc && rp.planes)
+      gathered = 8ull * ((data->num_graphs + 31ull) / 32ull) * 32ull * qg->pp.K * data->adj_words;
   }
   // per-query totals (and the matched pairs when a request asked for them)
   if (!rc && QG) {
@@ -407,6 +410,7 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
       o.ms_filter = mr.ms_signatures + mr.ms_filter;
       o.ms_mapping = mr.ms_mapping;
       o.ms_join = mr.ms_join;
+      o.gathered_plane_bytes = gathered;
       o.projected_bytes = reserved;
       o.pairs = static_cast<uint64_t>(r->num_queries) * data->num_graphs;
       if (!rc) {

@@ -353,25 +353,34 @@ def test_wildcard_join_matches_oracle(profile, wg):
 @pytest.mark.parametrize("extra", [[], ["--batched"]])
 def test_cli_driver_matches_oracle(tmp_path, extra):
     """The reference driver rewritten on the C++ API (sigmo_b200/sigmo_cli):
-    text files in, '# Matches' out, as SIGMo's log parser reads it."""
+    text files in, the full report out (candidate analysis included, the
+    per-query-vertex counts on stderr), read the way SIGMo's log parser reads
+    it (tests/cli_report.py restates scripts/utils/output_analyzer.py) and
+    compared with the oracle: graph and vertex counts, work-group size, the
+    candidate counts and their summary, refinement steps and matches."""
     import subprocess
     from pathlib import Path
+
+    from cli_report import expected_from_oracle, parse_report
 
     d = sb.generate_molecules(800, 10, 40, seed=4701)
     q = sb.generate_queries(25, 3, 10, seed=4702)
     (tmp_path / "d.dat").write_text(d.to_text())
     (tmp_path / "q.dat").write_text(q.to_text())
     cli = Path(sb.__file__).resolve().parent / "sigmo_cli"
+    qb, db = oracle.parse_text(q.to_text()), oracle.parse_text(d.to_text())
     for find_all in (True, False):
-        cmd = [str(cli), "-Q", str(tmp_path / "q.dat"), "-D", str(tmp_path / "d.dat"), "-i", "3", "--skip-candidates-analysis",
+        cmd = [str(cli), "-Q", str(tmp_path / "q.dat"), "-D", str(tmp_path / "d.dat"), "-i", "3", "-p",
                "--max-data-graphs", "1000000", "--max-query-graphs", "1000000"] + (["--find-all"] if find_all else []) + extra
         out = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
         assert out.returncode == 0, out.stderr
-        line = [l for l in out.stdout.splitlines() if l.startswith("# Matches:")][0]
-        got = int(line.split(":")[1].strip().replace(".", ""))
-        qb, db = oracle.parse_text(q.to_text()), oracle.parse_text(d.to_text())
-        want = oracle.run_pipeline(qb, db, 3, oracle.REF_PTX, not find_all)["total"]
-        assert got == want, (find_all, extra, got, want)
+        got = parse_report(out.stdout, out.stderr)
+        ref = oracle.run_pipeline(qb, db, 3, oracle.REF_PTX, not find_all)
+        want = expected_from_oracle(qb, db, ref["bits"], ref["total"], 3, find_all)
+        if extra:  # the batched pipeline prints one summary line instead of the per-step lines
+            want["n_refinement_steps"] = 0
+        for k, v in want.items():
+            assert got[k] == v, (find_all, extra, k)
 
 
 @pytest.mark.gpu
