@@ -12,7 +12,9 @@
  * on the NVIDIA PTX target it was written for are the parity contract:
  *   SIGMO_PROFILE_REF_PTX  (default) shift count >= width yields 0
  *   SIGMO_PROFILE_EXACT    exact sets, correct range masks, injective DFS
- *   SIGMO_PROFILE_REF_X86  accepted only by the CPU oracle (not this library)
+ *   SIGMO_PROFILE_REF_X86  shift count taken modulo the width (what the
+ *                          reference computes when built for an x86-64 host);
+ *                          stage-per-launch calls only
  */
 #ifndef SIGMO_B200_H
 #define SIGMO_B200_H

@@ -5,7 +5,7 @@ helpers (sigmo_b200/csrc/generator.cpp, host_graphs.cpp) compiled with g++
 alone.  bench.py's reference arm makes its inputs here, so that arm maps the
 oracle and this host library but never the product's CUDA library; the graphs
 are identical to sigmo_b200.generate_molecules / generate_queries for the same
-arguments (tests/test_oracle_cpu.py checks that).  Batches come back as
+arguments (tests/test_abi_cpu.py checks that).  Batches come back as
 oracle.Batch (numpy copies).
 """
 from __future__ import annotations
@@ -102,3 +102,19 @@ def slice_graphs(b: Batch, first: int, count: int) -> Batch:
                  (b.row_offsets[v0:v1 + 1] - np.uint32(e0)).astype(np.uint32),
                  (b.column_indices[e0:e1] - np.uint32(v0)).astype(np.uint32),
                  b.node_labels[v0:v1].copy(), b.edge_labels[e0:e1].copy())
+
+
+def format_text(b: Batch) -> str:
+    """The batch in the reference's text format, one graph per line
+    (sigmo_format_graphs; scripts/smile2graph.py:173-180 writes the same)."""
+    arrs = [np.ascontiguousarray(b.graph_offsets, np.uint32), np.ascontiguousarray(b.row_offsets, np.uint32),
+            np.ascontiguousarray(b.column_indices, np.uint32), np.ascontiguousarray(b.node_labels, np.uint8),
+            np.ascontiguousarray(b.edge_labels, np.uint8)]
+    raw = _HostGraphsC(b.num_graphs, b.total_nodes, b.total_edges, *[a.ctypes.data for a in arrs])
+    L = lib()
+    L.sigmo_format_graphs.argtypes = [ctypes.POINTER(_HostGraphsC), ctypes.c_char_p, ctypes.POINTER(ctypes.c_size_t)]
+    n = ctypes.c_size_t(0)
+    _check(L.sigmo_format_graphs(ctypes.byref(raw), None, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    _check(L.sigmo_format_graphs(ctypes.byref(raw), buf, ctypes.byref(n)))
+    return buf.raw[: n.value].decode()

@@ -208,8 +208,8 @@ int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out
   sigmo_options o;
   sigmo_default_options(&o);
   if (opts) o = *opts;
-  if (o.profile != SIGMO_PROFILE_REF_PTX && o.profile != SIGMO_PROFILE_EXACT)
-    return fail(SIGMO_ERR_INVALID, "profile %d is not supported on the device (REF_X86 is oracle-only)", o.profile);
+  if (o.profile != SIGMO_PROFILE_REF_PTX && o.profile != SIGMO_PROFILE_EXACT && o.profile != SIGMO_PROFILE_REF_X86)
+    return fail(SIGMO_ERR_INVALID, "unknown semantics profile %d", o.profile);
   if (o.join_work_group_size == 0) o.join_work_group_size = 128;
   if (o.join_work_group_size > 1024 || (o.join_work_group_size & 31u))
     return fail(SIGMO_ERR_INVALID, "join work-group size %u must be a multiple of 32 <= 1024", o.join_work_group_size);
@@ -778,6 +778,8 @@ int sigmo_join_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t da
 // off the driver path (sigmo.cpp never calls it).
 int sigmo_join_wildcard_candidates(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_t data, sigmo_candidates_t c, sigmo_gmcr_t m,
                           uint64_t* num_matches, int find_first, uint64_t* per_pair) {
+  if (q && q->opts.profile == kProfileX86)
+    return fail(SIGMO_ERR_DOMAIN, "joinWildcardCandidates runs under the REF_PTX and EXACT profiles");
   if (!q || !query || !data || !c || !m || !num_matches) return fail(SIGMO_ERR_INVALID, "null argument");
   if (m->num_data_graphs != data->num_graphs || !m->offsets) return fail(SIGMO_ERR_INVALID, "GMCR was not generated for this data graph");
   SIGMO_TRY(set_device(q));

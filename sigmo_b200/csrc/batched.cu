@@ -623,6 +623,8 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   if (data->max_nodes > 64u * kMaxAdjWords)
     return fail(SIGMO_ERR_DOMAIN, "the batched form supports data graphs of up to %u vertices (largest: %u)", 64u * kMaxAdjWords,
                 data->max_nodes);
+  if (q->opts.profile == kProfileX86)
+    return fail(SIGMO_ERR_DOMAIN, "the batched form runs the REF_PTX and EXACT profiles; REF_X86 runs the stage-per-launch calls");
   SIGMO_CUDA_TRY(cudaSetDevice(q->device));
   const sigmo_tuning& tn = q->tune;
   const uint64_t key[7] = {query->stamp, data->stamp, R, static_cast<uint64_t>(find_first),

@@ -8,6 +8,7 @@
 namespace sigmo_b200 {
 
 constexpr int kProfilePtx = 0;    // SIGMO_PROFILE_REF_PTX
+constexpr int kProfileX86 = 1;    // SIGMO_PROFILE_REF_X86 (stage-per-launch form only)
 constexpr int kProfileExact = 2;  // SIGMO_PROFILE_EXACT
 constexpr uint8_t kWildcard = 255;        // types::WILDCARD_NODE (types.hpp:23)
 constexpr uint32_t kMaxQueryNodes = 64;   // join depth supported by this library
@@ -56,6 +57,9 @@ __device__ __forceinline__ uint32_t ge_sliced(uint32_t x0, uint32_t x1, uint32_t
 // ---- shift semantics -------------------------------------------------------
 __host__ __device__ __forceinline__ uint32_t shr32p(uint32_t v, uint32_t n) { return n >= 32u ? 0u : (v >> n); }
 __host__ __device__ __forceinline__ uint32_t shl32p(uint32_t v, uint32_t n) { return n >= 32u ? 0u : (v << n); }
+// x86-64 (SHL/SHR): the count is taken modulo the register width.
+__host__ __device__ __forceinline__ uint32_t shr32x(uint32_t v, uint32_t n) { return v >> (n & 31u); }
+__host__ __device__ __forceinline__ uint32_t shl32x(uint32_t v, uint32_t n) { return v << (n & 31u); }
 
 // Range mask of bitset word i for the graph range [s, e)
 // (CandidatesDevice::getCandidatesCount, candidates.hpp:91-99).  REF_PTX: an
@@ -72,6 +76,12 @@ __host__ __device__ __forceinline__ uint32_t range_mask(uint32_t i, uint32_t s, 
     return m << (lo - (i << 5));
   }
   uint32_t m = 0xFFFFFFFFu;
+  if (prof == kProfileX86) {  // REF_X86: an over-wide shift uses the count modulo 32
+    if (start_idx == end_idx - 1u) m = shl32x(shr32x(m, 32u - (e - s)), s & 31u);
+    else if (i == start_idx) m = shl32x(m, s & 31u);
+    else if (i == end_idx - 1u) m = shr32x(m, 32u - (e & 31u));
+    return m;
+  }
   if (start_idx == end_idx - 1u) m = shl32p(shr32p(m, 32u - (e - s)), s & 31u);
   else if (i == start_idx) m = shl32p(m, s & 31u);
   else if (i == end_idx - 1u) m = shr32p(m, 32u - (e & 31u));
@@ -89,6 +99,12 @@ __host__ __device__ __forceinline__ uint32_t refbit_pos(uint32_t x, uint32_t off
 __host__ __device__ __forceinline__ uint64_t refbit(uint32_t x, uint32_t off) {
   uint32_t c = refbit_pos(x, off);
   return c >= 64u ? 0ull : (1ull << c);
+}
+// The same bit under the given profile: REF_X86 takes the count modulo 64, so
+// the set acts on (x - off) mod 64.
+__host__ __device__ __forceinline__ uint64_t refbit_prof(uint32_t x, uint32_t off, int prof) {
+  if (prof == kProfileX86) return 1ull << (((x & 0xFFu) - off) & 63u);
+  return refbit(x, off);
 }
 
 }  // namespace sigmo_b200

@@ -81,6 +81,11 @@ __device__ uint64_t ptx_wide_ball(uint32_t v, uint32_t prev, uint32_t view, cons
 // refineCSRSignatures<PowerGraph> (signature.hpp:348-386), REF_PTX profile:
 // sphere = ball_view(v) \ {v} \ old(v); sig = label histogram of the sphere;
 // old |= sphere.  Local ids >= 64 have no bit (graph sizes <= 256).
+// X86 (REF_X86, graphs of <= 256 vertices): the 64-bit sets take local id
+// mod 64 (Bitset<uint64_t> with the shift count modulo 64), so a vertex's
+// neighbours land on their ids mod 64 (its adjacency words ORed together),
+// and the frontier's bit b expands vertex b of the graph.
+template <bool X86>
 __global__ void k_sig_refine_ptx(uint64_t N, const uint32_t* __restrict__ goff, const uint32_t* __restrict__ node_graph,
                                  const uint64_t* __restrict__ adj, uint32_t AW, const uint32_t* __restrict__ roff,
                                  const uint32_t* __restrict__ col, const uint8_t* __restrict__ lab, uint32_t view,
@@ -90,11 +95,11 @@ __global__ void k_sig_refine_ptx(uint64_t N, const uint32_t* __restrict__ goff, 
     const uint32_t g = node_graph[v];
     const uint32_t prev = goff[g], n = goff[g + 1] - prev;
     uint64_t self, R;
-    if (n > 256u) {
+    if (!X86 && n > 256u) {
       R = ptx_wide_ball(v, prev, view, roff, col, &self);
     } else {
       const uint32_t lv = v - prev;
-      self = lv < 64u ? (1ull << lv) : 0ull;
+      self = X86 ? (1ull << (lv & 63u)) : (lv < 64u ? (1ull << lv) : 0ull);
       uint64_t F = self;
       R = self;
       for (uint32_t it = 0; it < view && F; ++it) {
@@ -102,7 +107,12 @@ __global__ void k_sig_refine_ptx(uint64_t N, const uint32_t* __restrict__ goff, 
         while (m) {
           const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
           m &= m - 1;
-          nx |= adj[static_cast<uint64_t>(prev + b) * AW];
+          const uint64_t* row = adj + static_cast<uint64_t>(prev + b) * AW;
+          if (X86) {
+            for (uint32_t k = 0; k < AW; ++k) nx |= row[k];
+          } else {
+            nx |= row[0];
+          }
         }
         nx &= ~R;
         R |= nx;
@@ -392,8 +402,16 @@ int launch_sig_refine(Queue* q, const Graph* g, uint32_t view, uint64_t* sig, ui
     }
     return check_launch(q, "k_sig_refine_exact");
   }
-  k_sig_refine_ptx<<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->adj_words,
-                                                g->row_offsets, g->column_indices, g->node_labels, view, sig, reach);
+  if (q->opts.profile == kProfileX86) {
+    if (g->max_nodes > 64u * kMaxAdjWords)
+      return fail(SIGMO_ERR_DOMAIN, "REF_X86 profile supports graphs of at most %u vertices (largest: %u)", 64u * kMaxAdjWords,
+                  g->max_nodes);
+    k_sig_refine_ptx<true><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->adj_words,
+                                                        g->row_offsets, g->column_indices, g->node_labels, view, sig, reach);
+    return check_launch(q, "k_sig_refine_x86");
+  }
+  k_sig_refine_ptx<false><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->adj_words,
+                                                       g->row_offsets, g->column_indices, g->node_labels, view, sig, reach);
   return check_launch(q, "k_sig_refine_ptx");
 }
 

@@ -237,7 +237,9 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
             const uint32_t sh = s & 31u;
             const uint64_t lo = static_cast<uint64_t>(pc.w[qn][0]) | (static_cast<uint64_t>(pc.w[qn][1]) << 32);
             const uint64_t cm = (lo >> sh) | (sh ? (static_cast<uint64_t>(pc.w[qn][2]) << (64u - sh)) : 0ull);
-            const uint64_t low = s >= 256u ? 0ull : (256u - s >= 64u ? ~0ull : ((1ull << (256u - s)) - 1ull));
+            // REF_X86: every local bit is live (a <= 64-vertex graph's set is exact)
+            const uint64_t low = prof == kProfileX86 ? ~0ull
+                                 : (s >= 256u ? 0ull : (256u - s >= 64u ? ~0ull : ((1ull << (256u - s)) - 1ull)));
             uint64_t place = cm & vmask[qn] & ~visited;
             if (place) {
               if (find_first) place &= 0ull - place;
@@ -247,7 +249,7 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
               if (find_first) break;
             }
             --top;
-            visited &= ~refbit(mapping[qn], s);
+            visited &= ~refbit_prof(mapping[qn], s, prof);
             if (top == 1) visited = 0;
             if (budget_spent(lim, steps)) {
               stop = true;
@@ -257,7 +259,7 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
           }
           if (fr.idx >= count_of(qn)) {
             --top;
-            visited &= ~refbit(mapping[qn], s);
+            visited &= ~refbit_prof(mapping[qn], s, prof);
             if (top == 1) visited = 0;
             if (budget_spent(lim, steps)) {
               stop = true;
@@ -267,11 +269,11 @@ __global__ void k_join_literal(const uint32_t* __restrict__ bits, uint64_t Wp, i
           }
           const uint32_t cand = cand_of(qn, fr.idx);
           stack[top - 1].idx++;
-          if (visited & refbit(cand, s)) continue;
+          if (visited & refbit_prof(cand, s, prof)) continue;
           if (valid(qn, cand)) {
             mapping[qn] = cand;
             if (small) rowc[qn] = dadj[static_cast<uint64_t>(cand) * dAW];
-            visited |= refbit(cand, s);
+            visited |= refbit_prof(cand, s, prof);
             stack[top++] = {qn + 1, 0u};
             push_mask(qn + 1);
           }
@@ -402,9 +404,13 @@ __global__ void k_join_literal_small(const uint32_t* __restrict__ bits, uint64_t
     const uint8_t map0 = s == 0 ? 0 : kLitOutside;
 #pragma unroll 1
     for (uint32_t k = 0; k < kLitLevels; ++k) LV(map, k) = map0;  // mapping[] of a fresh work-item
-    // graph-local bits whose global id is below 256: the only ones the
-    // reference's uint8-indexed visited set can hold
-    const uint64_t low = s >= 256u ? 0ull : (256u - s >= 64u ? ~0ull : ((1ull << (256u - s)) - 1ull));
+    // graph-local bits the reference's uint8-indexed visited set can hold:
+    // under REF_PTX those whose global id is below 256; under REF_X86 all
+    // (the count modulo 64 is the local id).  A fresh work-item's mapping[]
+    // (global vertex 0) names under REF_X86 the bit (0 - s) mod 64.
+    const uint64_t low = prof == kProfileX86 ? ~0ull
+                         : (s >= 256u ? 0ull : (256u - s >= 64u ? ~0ull : ((1ull << (256u - s)) - 1ull)));
+    const uint64_t outside_bit = prof == kProfileX86 ? (1ull << ((0u - s) & 63u)) : 0ull;
     const uint32_t i0 = s >> 5, nw = ((e + 31u) >> 5) - i0, sh = s & 31u;
     for (uint32_t it = lid; it < seg1 - seg0; it += wg) {
       if (join_stopped(lim)) {
@@ -467,7 +473,7 @@ __global__ void k_join_literal_small(const uint32_t* __restrict__ bits, uint64_t
           if (top) visited &= ~(1ull << LV(map, top - 1));  // the parent's pick
         } else {
           const uint32_t mq = LV(map, qn);  // mapping[qn], perhaps stale
-          if (mq < 64u) visited &= ~((1ull << mq) & low);
+          visited &= ~(mq < 64u ? ((1ull << mq) & low) : outside_bit);
           if (top == 1) visited = 0;
         }
         if (budget_spent(lim, steps)) {

@@ -508,6 +508,8 @@ int sigmo_server_create(int device, const sigmo_host_graphs* database, const sig
   if (o.max_inflight == 0 || o.max_inflight > 16) return fail(SIGMO_ERR_INVALID, "max_inflight must be in 1..16");
   if (o.max_batch_queries == 0) return fail(SIGMO_ERR_INVALID, "max_batch_queries must be positive");
   if (o.iterations > 64) return fail(SIGMO_ERR_INVALID, "iterations must be <= 64");
+  if (opts && opts->profile == SIGMO_PROFILE_REF_X86)
+    return fail(SIGMO_ERR_DOMAIN, "the serving loop runs the REF_PTX and EXACT profiles");
   std::unique_ptr<sigmo_server_s> s(new (std::nothrow) sigmo_server_s());
   if (!s) return fail(SIGMO_ERR_OOM, "host allocation failed");
   s->device = device;
