@@ -16,15 +16,20 @@
 //                    size (<= 256 vertices per graph), correct range masks, an
 //                    injective DFS with clean backtracking.
 //
-// Pinning: the signature word layout, the candidate bit layout, the batched CSR
-// layout and the label filter are pinned by the reference's own known-answer
-// tests (library/test/candidates.cpp:13-32,119-143, library/test/graphs.cpp:
-// 59-120, library/test/filter.cpp:14-68) on its fixtures
-// (library/test/data/test_{data,query}.dat).  The PowerGraph refinement, GMCR
-// and the join have no surviving reference test; they are cross-checked against
-// an independent pure-Python restatement (tests/pyref.py) and a brute-force
-// subgraph counter, so for those stages parity is pinned only by restatement.
-//
+// Pinning: the reference's own hot-path code (library/include/*.hpp) is built
+// for the host by oracle/ref_build.py (g++ with the SYCL stand-in
+// oracle/sycl_host) and run on seeded inputs; its signatures and candidate
+// bitsets after the filter and after every refinement, its GMCR and its
+// find-all / find-first totals equal this oracle's ORC_REF_X86 profile
+// (tests/test_ref_cpu.py, against the live build and against the committed
+// outputs tests/golden/ref_golden.json).  ORC_REF_PTX shares every line with
+// ORC_REF_X86 except the three shift helpers below (shl64_one, shl32, shr32);
+// ORC_EXACT takes its own branches (exact sets and range masks, an injective
+// DFS) and is checked against a brute-force embedding count.  The reference's own
+// known-answer tests (library/test/candidates.cpp:13-32,119-143,
+// library/test/graphs.cpp:59-120, library/test/filter.cpp:14-68) are checked
+// too (tests/test_oracle_cpu.py).
+
 // Build: oracle/Makefile -> oracle/liboracle_sigmo.so (g++ -O3 -fopenmp).
 
 #include <algorithm>
