@@ -550,7 +550,8 @@ def run_sigmo(args, rank, world, local):
                 queue.wait()
                 refine_ms.append(ev.getProfilingInfo() * 1e3)
             g2 = sb.GMCR(queue)
-            g2.generateGMCR(qg, dg, c2)
+            gev = g2.generateGMCR(qg, dg, c2)
+            gmcr_ms.append(gev.getProfilingInfo() * 1e3)
             nm = np.zeros(1, np.uint64)
             sb.joinCandidates(queue, qg, dg, c2, g2, nm, ff)
             queue.wait()
@@ -561,9 +562,10 @@ def run_sigmo(args, rank, world, local):
             g2.close()
             return int(nm[0]), dig, adm
 
-        refine_ms = []
+        refine_ms, gmcr_ms = [], []
         plain_step()  # warm-up
         refine_ms.clear()
+        gmcr_ms.clear()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.plain_steps):
@@ -576,13 +578,21 @@ def run_sigmo(args, rank, world, local):
         rb = refine_bytes(qg.total_nodes, dg.total_nodes)
         r_ms = statistics.median(refine_ms)
         r_ach = rb / (r_ms / 1e3) / 1e9
+        gb = 4 * qg.total_nodes * ((dg.total_nodes + 31) // 32) + 8 * dg.num_graphs
+        g_ms = statistics.median(gmcr_ms)
+        g_ach = gb / (g_ms / 1e3) / 1e9
         plain = {"value": pairs / (p_ms / 1e3), "unit": "pairs/s", "ms_per_step": round(p_ms, 3),
                  "batched_over_plain": round((pairs / (ms_per_step / 1e3)) / (pairs / (p_ms / 1e3)), 3),
                  "identical_results": bool(p_total == total_matches and p_adm == admitted),
                  "roofline_refine": {"kernel": "k_sig_planes + k_refine (one refinement pass)", "bound": "hbm",
                                      "achieved": round(r_ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(r_ach / hbm, 4),
                                      "traffic": traffic_for("k_refine", args.workload),
-                                     "algorithmic_bytes_per_launch": rb, "ms_per_launch": round(r_ms, 4)}}
+                                     "algorithmic_bytes_per_launch": rb, "ms_per_launch": round(r_ms, 4)},
+                 "roofline_gmcr": {"kernel": "GMCR stage (k_gmcr_ne's one read of the final bitset, admission, scan, "
+                                             "fill; stage events, so the fraction is a lower bound for k_gmcr_ne)",
+                                   "bound": "hbm", "achieved": round(g_ach, 1), "peak": hbm, "unit": "GB/s",
+                                   "frac": round(g_ach / hbm, 4), "algorithmic_bytes_per_launch": gb,
+                                   "ms_per_launch": round(g_ms, 4)}}
 
     # ---- e2e through the C ABI from pinned host buffers ----
     e2e = None

@@ -46,16 +46,35 @@ __global__ void k_gmcr_ne(const uint32_t* __restrict__ bits, uint64_t Wp, uint64
   }
   const uint64_t j0 = static_cast<uint64_t>(blockIdx.y) * kNeRowsPerBlock;
   const uint64_t j1 = j0 + kNeRowsPerBlock < Qn ? j0 + kNeRowsPerBlock : Qn;
+  // The range masks of this graph's words are the same for every row: a graph
+  // of <= 65 vertices spans at most kNeWords words, whose masks are computed
+  // once (a zero mask, REF_PTX's dropped last word, is not even loaded).
+  constexpr uint32_t kNeWords = 3;
+  const bool few = i1 - i0 <= kNeWords;
+  uint32_t mk[kNeWords];
+#pragma unroll
+  for (uint32_t w = 0; w < kNeWords; ++w) mk[w] = few && i0 + w < i1 ? range_mask(i0 + w, s, e, prof) : 0u;
   for (uint64_t j = j0; j < j1; j += kNeBatch) {
     uint32_t acc[kNeBatch];
 #pragma unroll
     for (uint32_t k = 0; k < kNeBatch; ++k) acc[k] = 0;
-    for (uint32_t i = i0; i < i1; ++i) {
-      const uint32_t m = range_mask(i, s, e, prof);
-      const uint32_t* col = bits + j * Wp + i;
+    if (few) {
 #pragma unroll
-      for (uint32_t k = 0; k < kNeBatch; ++k)
-        if (j + k < j1) acc[k] |= col[k * Wp] & m;
+      for (uint32_t w = 0; w < kNeWords; ++w) {
+        if (!mk[w]) continue;
+        const uint32_t* col = bits + j * Wp + i0 + w;
+#pragma unroll
+        for (uint32_t k = 0; k < kNeBatch; ++k)
+          if (j + k < j1) acc[k] |= col[k * Wp] & mk[w];
+      }
+    } else {
+      for (uint32_t i = i0; i < i1; ++i) {
+        const uint32_t m = range_mask(i, s, e, prof);
+        const uint32_t* col = bits + j * Wp + i;
+#pragma unroll
+        for (uint32_t k = 0; k < kNeBatch; ++k)
+          if (j + k < j1) acc[k] |= col[k * Wp] & m;
+      }
     }
 #pragma unroll
     for (uint32_t k = 0; k < kNeBatch; ++k) {

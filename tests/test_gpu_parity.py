@@ -388,7 +388,8 @@ def test_cli_driver_matches_oracle(tmp_path, extra):
 def test_shards_keep_the_unsharded_results(ff):
     """Data graphs split into contiguous shards (global vertex ids kept as a
     vertex base): the shards' GMCR segments and per-pair counts, concatenated,
-    are the unsharded run's.  REF_PTX, where results depend on global ids."""
+    are the unsharded run's, which are the oracle's.  REF_PTX, where results
+    depend on global ids."""
     d = sb.generate_molecules(6000, 10, 60, seed=4801)
     q = sb.generate_queries(60, 3, 20, seed=4802, skew_lo=5, skew_hi=12)
     queue = sb.Queue(0)
@@ -417,6 +418,10 @@ def test_shards_keep_the_unsharded_results(ff):
         seg_cnt.append(gms.getPairCounts())
     assert tot == full["total_matches"]
     assert np.array_equal(np.concatenate(seg_idx), idx) and np.array_equal(np.concatenate(seg_cnt), counts)
+    # and the unsharded run is the oracle's
+    ref = _oracle(q, d, 5, oracle.REF_PTX, ff)
+    assert np.array_equal(off, ref["offsets"]) and np.array_equal(idx, ref["indices"])
+    assert np.array_equal(counts, ref["per_pair"]) and full["total_matches"] == ref["total"]
     with pytest.raises(sb.SigmoError):
         sb.createDeviceCSRGraph(queue, d.slice(10, 5)).set_vertex_base(100)
 
