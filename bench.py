@@ -87,8 +87,8 @@ def parse_args():
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean request arrivals per second (Poisson)")
     ap.add_argument("--serve-mols", type=int, default=5_000_000,
                     help="serving database size (molecules of 10-40 atoms; 0: the workload's molecules)")
-    ap.add_argument("--serve-rate-low", type=float, default=20.0,
-                    help="a second serving run at this arrival rate (0: skip it)")
+    ap.add_argument("--serve-rates-low", default="20,40,60,80",
+                    help="further serving runs at these arrival rates (comma list; empty: none): where p99 <= 50 ms holds")
     ap.add_argument("--serve-inflight", type=int, default=2)
     ap.add_argument("--serve-batch-queries", type=int, default=64, help="most query graphs batched together")
     ap.add_argument("--no-graph", action="store_true", help="time ordinary calls instead of CUDA-graph replays")
@@ -331,7 +331,8 @@ def run_serving(args, d, wl, local):
     1-64 query graphs (3-30 atoms, skewed 6-15), find-first, continuous
     batching; latency = submit -> per-query results on the host, measured
     inside the library.  Runs at `--serve-rate` (the target rate, 200/s) and at
-    `--serve-rate-low`, each for `--serve-seconds` of arrivals, on one server."""
+    each of `--serve-rates-low`, each for `--serve-seconds` of arrivals, on one
+    server."""
     import threading
 
     import sigmo_b200 as sb
@@ -408,8 +409,11 @@ def run_serving(args, d, wl, local):
         }
 
     runs = {"target_rate": one_rate(args.serve_rate, 4242)}
-    if args.serve_rate_low > 0:
-        runs["low_rate"] = one_rate(args.serve_rate_low, 4343)
+    lows = [float(x) for x in args.serve_rates_low.split(",") if x.strip()]
+    if lows:
+        runs["lower_rates"] = [one_rate(rate, 4343 + i) for i, rate in enumerate(lows)]
+        held = [r["arrival_rate_per_s"] for r in runs["lower_rates"] if r["meets_target"]]
+        runs["highest_rate_meeting_target"] = max(held) if held else None
     st = srv.stats()
     srv.close()
     return {
