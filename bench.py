@@ -93,8 +93,9 @@ def parse_args():
     ap.add_argument("--serve-batch-queries", type=int, default=64, help="most query graphs batched together")
     ap.add_argument("--no-graph", action="store_true", help="time ordinary calls instead of CUDA-graph replays")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default join launch shape")
-    ap.add_argument("--join-kernel", type=int, choices=[0, 1], default=None,
-                    help="force the join kernel (0: per-lane DFS, 1: warp-cooperative frontier) after any autotuning")
+    ap.add_argument("--join-kernel", type=int, choices=[0, 1, 2], default=None,
+                    help="force the join kernel (2: per-lane DFS with CTA-local slot regions, the default; 0: per-lane DFS "
+                         "with one work cursor; 1: warp-cooperative frontier) after any autotuning")
     ap.add_argument("--serving-only", action="store_true", help="run only the serving measurement (prints its JSON)")
     ap.add_argument("--shard", action="store_true",
                     help="N>1: split one workload's molecules over the ranks (strong scaling, global ids kept) instead of "
@@ -279,6 +280,9 @@ def peaks():
         j = json.loads(p.read_text())
         return float(j["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+JOIN_KERNELS = {0: "k_join_masks", 1: "k_join_frontier", 2: "k_join_lanes"}  # sigmo_tuning.join_kernel
 
 
 def traffic_for(kernel: str, workload: str, key: str = "bytes_per_launch"):
@@ -518,22 +522,25 @@ def run_sigmo(args, rank, world, local):
     jb = join_bytes(q, d, offsets, indices)
     join_ms = med("ms_join")
     achieved = jb / (join_ms / 1e3) / 1e9
-    roof = {"kernel": "join stage: k_pair_masks + k_join_masks (side stream: k_join_fast for queries over 16 vertices, "
-                      "k_join_literal for the data graphs starting below vertex 256)",
+    jk = JOIN_KERNELS.get(queue.get_tuning()["join_kernel"], "k_join_lanes")
+    jkey = f"join:{jk}"
+    l1, l2 = traffic_for(jkey, args.workload, "l1_hit_rate"), traffic_for(jkey, args.workload, "l2_hit_rate")
+    roof = {"kernel": f"join stage: k_pair_masks + {jk} (side stream: k_join_fast for queries over 16 vertices, "
+                      "k_join_literal_small for the data graphs starting below vertex 256)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-            "frac": round(achieved / hbm, 4), "traffic": traffic_for("join", args.workload),
+            "frac": round(achieved / hbm, 4), "traffic": traffic_for(jkey, args.workload),
             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured" else peak_kind,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the join kernels on a 20,000-molecule "
-                              "slice of this workload, scaled to this batch by admitted pairs (profiles/traffic.json); "
-                              "the join counters below come from the same capture",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_pair_masks and the phase-B kernel "
+                              "on a 20,000-molecule slice of this workload, scaled to this batch by admitted pairs "
+                              "(profiles/traffic.json); the phase-B counters below come from the same capture",
             "algorithmic_bytes_per_launch": jb, "ms_per_launch": round(join_ms, 4),
-            "warp_execution_efficiency": traffic_for("join", args.workload, "warp_execution_efficiency"),
-            "active_warps_of_peak": traffic_for("join", args.workload, "active_warps_of_peak"),
-            "issue_active_of_peak": traffic_for("join", args.workload, "issue_active_of_peak"),
-            "note": "DFS over admitted pairs: latency-bound, no bandwidth roofline applies (ncu: threads per "
-                    "instruction / 32, active warps and issue-active fraction above; 92 % of its loads hit L2); "
-                    "the stage is "
-                    f"{100 * join_ms / stages['ms_total']:.0f}% of the step"}
+            "warp_execution_efficiency": traffic_for(jkey, args.workload, "warp_execution_efficiency"),
+            "active_warps_of_peak": traffic_for(jkey, args.workload, "active_warps_of_peak"),
+            "issue_active_of_peak": traffic_for(jkey, args.workload, "issue_active_of_peak"),
+            "note": "DFS over admitted pairs: latency- and issue-bound, no bandwidth roofline applies (ncu: threads "
+                    "per instruction / 32, active warps and issue-active fraction above"
+                    + (f"; L1 hit rate {l1:.0%}, L2 hit rate {l2:.0%}" if l1 is not None and l2 is not None else "")
+                    + f"); the stage is {100 * join_ms / stages['ms_total']:.0f}% of the step"}
 
     # ---- the plain stage-per-launch form (same results, reference order) ----
     plain = None

@@ -123,15 +123,21 @@ SIGMO_API void sigmo_default_options(sigmo_options* o);
  * the defaults (overflow_serial and join_kernel: 0 is a value).  sigmo_autotune
  * searches these on a caller's own workload. */
 typedef struct sigmo_tuning {
-  uint32_t join_blocks_per_sm;   /* persistent join CTAs per SM, 1..3 (3)                      */
-  uint32_t join_chunk;           /* GMCR slots a lane takes per work grab, 1..64 (4)             */
+  uint32_t join_blocks_per_sm;   /* persistent join CTAs per SM, 1..4 (4; join_kernel 0 and 1
+                                    keep at most 3 resident)                                    */
+  uint32_t join_chunk;           /* GMCR slots a lane takes per work grab, 1..64 (4; join_kernel
+                                    0 and 1)                                                    */
   uint32_t overflow_blocks;      /* CTAs of the join for queries over 16 vertices (1184)        */
   uint32_t overflow_serial;      /* 0 (default): run those beside the main join; 1: after it       */
   uint32_t mask_chunk_slots;     /* GMCR slots per level-mask pass, in 2^20 units, 1..64 (8)     */
   uint32_t overflow_split;       /* work items per pair of those queries, each taking every
                                     split-th root candidate, 1..64 (16)                          */
-  uint32_t join_kernel;          /* 0 (default): per-lane DFS machine; 1: warp-cooperative
-                                    frontier join (32 candidate tries per round, one per lane)   */
+  uint32_t join_kernel;          /* 2 (default): per-lane DFS with 9 B of shared state per level
+                                    and CTA-local slot regions; 0: per-lane DFS with 17 B per
+                                    level and one work cursor; 1: warp-cooperative frontier join
+                                    (32 candidate tries per round, one per lane)                 */
+  uint32_t join_pool;            /* join_kernel 2: sixteenths of the slots in the pool shared by
+                                    all CTAs after their own regions, 1..16 (2)                  */
 } sigmo_tuning;
 /* sycl::queue{gpu_selector_v, enable_profiling} (library/src/sigmo.cpp:19). */
 SIGMO_API int sigmo_queue_create(int device, const sigmo_options* opts, sigmo_queue_t* out);

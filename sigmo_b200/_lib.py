@@ -53,6 +53,7 @@ class TuningC(ctypes.Structure):
         ("mask_chunk_slots", ctypes.c_uint32),
         ("overflow_split", ctypes.c_uint32),
         ("join_kernel", ctypes.c_uint32),
+        ("join_pool", ctypes.c_uint32),
     ]
 
 

@@ -17,19 +17,21 @@
 namespace sigmo_b200 {
 
 int normalize_tuning(sigmo_tuning* t) {
-  const sigmo_tuning d{3, 4, 148 * 8, 0, 8, 16, 0};
+  const sigmo_tuning d = Queue{}.tune;
   if (!t->join_blocks_per_sm) t->join_blocks_per_sm = d.join_blocks_per_sm;
   if (!t->join_chunk) t->join_chunk = d.join_chunk;
   if (!t->overflow_blocks) t->overflow_blocks = d.overflow_blocks;
   if (!t->mask_chunk_slots) t->mask_chunk_slots = d.mask_chunk_slots;
   if (!t->overflow_split) t->overflow_split = d.overflow_split;
-  if (t->join_blocks_per_sm > 3) return fail(SIGMO_ERR_INVALID, "join_blocks_per_sm must be 1..3");
+  if (!t->join_pool) t->join_pool = d.join_pool;
+  if (t->join_blocks_per_sm > 4) return fail(SIGMO_ERR_INVALID, "join_blocks_per_sm must be 1..4");
   if (t->join_chunk > 64) return fail(SIGMO_ERR_INVALID, "join_chunk must be 1..64");
   if (t->overflow_blocks > 65535) return fail(SIGMO_ERR_INVALID, "overflow_blocks must be <= 65535");
   if (t->overflow_serial > 1) return fail(SIGMO_ERR_INVALID, "overflow_serial must be 0 or 1");
   if (t->mask_chunk_slots > 64) return fail(SIGMO_ERR_INVALID, "mask_chunk_slots must be 1..64");
   if (t->overflow_split > 64) return fail(SIGMO_ERR_INVALID, "overflow_split must be 1..64");
-  if (t->join_kernel > 1) return fail(SIGMO_ERR_INVALID, "join_kernel must be 0 or 1");
+  if (t->join_kernel > 2) return fail(SIGMO_ERR_INVALID, "join_kernel must be 0, 1 or 2");
+  if (t->join_pool > 16) return fail(SIGMO_ERR_INVALID, "join_pool must be 1..16");
   return SIGMO_OK;
 }
 

@@ -630,7 +630,7 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   const uint64_t key[7] = {query->stamp, data->stamp, R, static_cast<uint64_t>(find_first),
                            static_cast<uint64_t>(q->opts.profile) | (static_cast<uint64_t>(tn.overflow_serial) << 8) |
                                (static_cast<uint64_t>(tn.overflow_split) << 16) |
-                               (static_cast<uint64_t>(tn.join_kernel) << 24),
+                               (static_cast<uint64_t>(tn.join_kernel) << 24) | (static_cast<uint64_t>(tn.join_pool) << 32),
                            (static_cast<uint64_t>(tn.join_blocks_per_sm) << 48) | (static_cast<uint64_t>(tn.join_chunk) << 40) |
                                (static_cast<uint64_t>(tn.mask_chunk_slots) << 32) | tn.overflow_blocks,
                            q->join_budget};
@@ -750,9 +750,10 @@ extern "C" int sigmo_autotune(sigmo_queue_t q, sigmo_graph_t query, sigmo_graph_
     std::vector<uint32_t> values;
   };
   const Axis axes[] = {
-      {&sigmo_tuning::join_kernel, {0, 1}},
+      {&sigmo_tuning::join_kernel, {0, 1, 2}},
       {&sigmo_tuning::overflow_serial, {0, 1}},
-      {&sigmo_tuning::join_blocks_per_sm, {1, 2, 3}},
+      {&sigmo_tuning::join_blocks_per_sm, {1, 2, 3, 4}},
+      {&sigmo_tuning::join_pool, {1, 2, 4, 8}},
       {&sigmo_tuning::join_chunk, {1, 2, 4, 8, 16}},
       {&sigmo_tuning::overflow_blocks, {148, 296, 592, 1184, 2368}},
       {&sigmo_tuning::mask_chunk_slots, {2, 8, 32}},

@@ -33,7 +33,7 @@ struct Queue {
   int device = 0;
   cudaStream_t stream = nullptr;
   sigmo_options opts{};
-  sigmo_tuning tune{3, 4, 148 * 8, 0, 8, 16, 0};
+  sigmo_tuning tune{4, 4, 148 * 8, 0, 8, 16, 2, 2};
   cudaEvent_t ev_start = nullptr, ev_end = nullptr;
   bool stage_recorded = false;
   uint64_t launches = 0;

@@ -21,7 +21,7 @@ def _symmetric_case():
     return q, d
 
 
-@pytest.mark.parametrize("join_kernel", [0, 1])
+@pytest.mark.parametrize("join_kernel", [0, 1, 2])
 @pytest.mark.parametrize("prof", ["ref-ptx", "exact"])
 def test_budget_spent_returns_timeout_and_queue_recovers(join_kernel, prof):
     q, d = _symmetric_case()

@@ -48,12 +48,17 @@ def run_plain(qh, dh, R, profile, find_first, wg=128, keep=False):
     return hist
 
 
-def run_batched(qh, dh, R, profile, find_first, wg=128, keep_bits=False, join_kernel=0):
+def run_batched(qh, dh, R, profile, find_first, wg=128, keep_bits=False, join_kernel=None, **tuning):
     """keep_bits: the bitset route (final bitset materialised); otherwise the
-    plane route, which never writes the bitset.  join_kernel: 0 the per-lane
-    DFS machine, 1 the warp-cooperative frontier join."""
+    plane route, which never writes the bitset.  join_kernel: None the
+    library default (2, the per-lane DFS with CTA-local slot regions), 0 the
+    per-lane DFS machine with one work cursor, 1 the warp-cooperative frontier
+    join; further tuning fields by name."""
     queue = sb.Queue(0, profile=profile, join_work_group_size=wg)
-    queue.set_tuning(join_kernel=join_kernel)
+    if join_kernel is not None:
+        tuning["join_kernel"] = join_kernel
+    if tuning:
+        queue.set_tuning(**tuning)
     qg, dg = sb.createDeviceCSRGraph(queue, qh), sb.createDeviceCSRGraph(queue, dh)
     cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes) if keep_bits else None
     gm = sb.GMCR(queue)
@@ -190,14 +195,23 @@ def test_symmetry_stress_small(prof):
     assert ref["per_pair"].max() >= 12  # automorphic patterns give many embeddings
 
 
+JOIN_SHAPES = [
+    dict(join_kernel=1),  # warp-cooperative frontier join
+    dict(join_kernel=0),  # per-lane DFS machine, one work cursor
+    dict(join_kernel=2, join_pool=16, join_blocks_per_sm=3),  # CTA regions off: every slot from the shared pool
+    dict(join_kernel=2, join_pool=1, join_blocks_per_sm=1),  # nearly all slots from the CTAs' own regions
+]
+
+
 @pytest.mark.parametrize("prof", DEVICE_PROFILES)
 @pytest.mark.parametrize("ff", [False, True])
-def test_frontier_join_matches_oracle(prof, ff):
-    """The warp-cooperative frontier join (join_kernel=1) gives the oracle's
-    GMCR and per-pair counts: drug-like pairs, queries over 16 vertices and
-    molecules over 64 atoms (both take the generic kernel), and automorphic
-    queries on ring-rich molecules (thousands of embeddings per pair, the
-    deepest frontier levels)."""
+@pytest.mark.parametrize("shape", range(len(JOIN_SHAPES)))
+def test_join_kernels_match_oracle(prof, ff, shape):
+    """Every join phase-B kernel and work split gives the oracle's GMCR and
+    per-pair counts: drug-like pairs, queries over 16 vertices and molecules
+    over 64 atoms (both take the generic kernel), and automorphic queries on
+    ring-rich molecules (thousands of embeddings per pair, the deepest DFS
+    levels); the default shape gives the same counts."""
     cases = [
         (sb.generate_molecules(1500, 10, 60, seed=5101), sb.generate_queries(120, 3, 24, seed=5102, skew_lo=6, skew_hi=15), 6),
         (sb.generate_molecules(400, 6, 120, seed=5103, kind=1, median=30), sb.generate_queries(30, 3, 14, seed=5104), 4),
@@ -205,7 +219,7 @@ def test_frontier_join_matches_oracle(prof, ff):
     ]
     for i, (dh, qh, R) in enumerate(cases):
         ref = _oracle(qh, dh, R, prof, ff)
-        out = run_batched(qh, dh, R, prof, ff, join_kernel=1)
+        out = run_batched(qh, dh, R, prof, ff, **JOIN_SHAPES[shape])
         _check(out, ref, f"case {i}")
         assert np.array_equal(out["per_pair"], run_batched(qh, dh, R, prof, ff)["per_pair"]), f"case {i}"
     assert ref["per_pair"].max() >= (1 if ff else 12)

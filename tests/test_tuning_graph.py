@@ -56,7 +56,7 @@ def test_autotune_keeps_results_and_sets_the_queue():
     assert t["ms_join"] <= t["ms_join_default"] * 1.05
     got = queue.get_tuning()
     for k in ("join_blocks_per_sm", "join_chunk", "overflow_blocks", "overflow_serial", "mask_chunk_slots", "overflow_split",
-              "join_kernel"):
+              "join_kernel", "join_pool"):
         assert got[k] == t[k]
     after = sb.match_batched(queue, qg, dg, R, False, None, sb.GMCR(queue))
     assert after["total_matches"] == base["total_matches"]
@@ -69,16 +69,20 @@ def test_autotune_keeps_results_and_sets_the_queue():
         assert r["total_matches"] == base["total_matches"]
         f = sb.match_batched(queue, qg, dg, R, True, None, gm)
         assert f["total_matches"] == base_ff["total_matches"]
-    # the frontier join under graph replay
-    queue.set_tuning(join_kernel=1, join_blocks_per_sm=3, join_chunk=4, mask_chunk_slots=8, overflow_split=16)
-    gm = sb.GMCR(queue)
-    for _ in range(3):
-        r = sb.match_batched(queue, qg, dg, R, False, None, gm, graph=True)
-        assert r["total_matches"] == base["total_matches"]
+    # every phase-B kernel under graph replay, the default one with CTA regions and without
+    for shape in (dict(join_kernel=1, join_blocks_per_sm=3), dict(join_kernel=0, join_blocks_per_sm=3),
+                  dict(join_kernel=2, join_blocks_per_sm=4, join_pool=2), dict(join_kernel=2, join_blocks_per_sm=4, join_pool=16)):
+        queue.set_tuning(join_chunk=4, mask_chunk_slots=8, overflow_split=16, **shape)
+        gm = sb.GMCR(queue)
+        for _ in range(3):
+            r = sb.match_batched(queue, qg, dg, R, False, None, gm, graph=True)
+            assert r["total_matches"] == base["total_matches"], shape
     with pytest.raises(sb.SigmoError):
         queue.set_tuning(join_blocks_per_sm=9)
     with pytest.raises(sb.SigmoError):
-        queue.set_tuning(join_kernel=2)
+        queue.set_tuning(join_kernel=3)
+    with pytest.raises(sb.SigmoError):
+        queue.set_tuning(join_pool=17)
 
 
 def test_graph_mode_exact_profile():
