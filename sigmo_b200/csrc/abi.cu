@@ -83,6 +83,49 @@ int dev_alloc(Queue* q, void** p, size_t bytes) {
 void dev_free(Queue* q, void* p) {
   if (p) cudaFreeAsync(p, q->stream);
 }
+
+namespace {
+// One pool per device for per-call temporaries; its release threshold is
+// unlimited, so freed blocks stay mapped for the next call.
+int tmp_pool(int device, cudaMemPool_t* out) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, cudaMemPool_t>> pools;
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto& d : pools)
+    if (d.first == device) {
+      *out = d.second;
+      return SIGMO_OK;
+    }
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  SIGMO_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+  uint64_t threshold = UINT64_MAX;
+  SIGMO_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+  pools.emplace_back(device, pool);
+  *out = pool;
+  return SIGMO_OK;
+}
+}  // namespace
+
+int tmp_alloc(Queue* q, void** p, size_t bytes) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  SIGMO_CUDA_TRY(cudaStreamIsCapturing(q->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return dev_alloc(q, p, bytes);
+  *p = nullptr;
+  cudaMemPool_t pool = nullptr;
+  SIGMO_TRY(tmp_pool(q->device, &pool));
+  cudaError_t e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, q->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(e == cudaErrorMemoryAllocation ? SIGMO_ERR_OOM : SIGMO_ERR_CUDA, "device allocation of %zu bytes failed: %s",
+                bytes, cudaGetErrorString(e));
+  }
+  return SIGMO_OK;
+}
 int queue_scratch(Queue* q, size_t bytes, void** p) {
   if (bytes > q->scratch_bytes) {
     dev_free(q, q->scratch);

@@ -391,7 +391,7 @@ int batched_bitset(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   void* buf = nullptr;
   const uint64_t b_dsig = run.dsig ? 0 : 8ull * R * N, b_planes = 16ull * 16 * R * c->Wp;
   auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-  SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + 256));
+  SIGMO_TRY(tmp_alloc(q, &buf, al(b_dsig) + al(b_planes) + 256));
   uint64_t* dsig = run.dsig ? const_cast<uint64_t*>(run.dsig) : static_cast<uint64_t*>(buf);
   uint32_t* planes = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + al(b_dsig));
   int rc = run.dsig ? SIGMO_OK : launch_sig_all(q, data, R, dsig);
@@ -452,7 +452,7 @@ int batched_planes(Queue* q, Graph* query, Graph* data, uint32_t R, int find_fir
   const uint64_t b_map = 4ull * row_map.size() + 2ull * rprog.size();
   const uint64_t b_lplanes = 16ull * 16 * R * Wlp, b_lbits = 4ull * Qn * Wlp;
   void* buf = nullptr;
-  SIGMO_TRY(dev_alloc(q, &buf, al(b_dsig) + al(b_planes) + al(b_ne) + al(b_lplanes) + al(b_lbits) + al(b_map) + 256));
+  SIGMO_TRY(tmp_alloc(q, &buf, al(b_dsig) + al(b_planes) + al(b_ne) + al(b_lplanes) + al(b_lbits) + al(b_map) + 256));
   char* p = static_cast<char*>(buf);
   uint64_t* dsig = run.dsig ? const_cast<uint64_t*>(run.dsig) : reinterpret_cast<uint64_t*>(p);
   p += al(b_dsig);
@@ -587,7 +587,7 @@ int capture_graph(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   SIGMO_CUDA_TRY(cudaStreamBeginCapture(q->stream, cudaStreamCaptureModeThreadLocal));
   uint64_t* d_total = nullptr;
   int rc = join_status_reset(q);
-  if (!rc) rc = dev_alloc(q, reinterpret_cast<void**>(&d_total), 8);
+  if (!rc) rc = tmp_alloc(q, reinterpret_cast<void**>(&d_total), 8);
   if (!rc && cudaMemsetAsync(d_total, 0, 8, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
   if (!rc) rc = batched_planes(q, query, data, R, find_first, m, d_total, ev, run);
   uint64_t* pin = static_cast<uint64_t*>(q->pinned);
@@ -646,7 +646,7 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   SIGMO_CUDA_TRY(cudaEventRecord(ev.e[0], q->stream));
   SIGMO_TRY(build_plane_program(q, query, R));
   uint64_t* d_total = nullptr;
-  SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&d_total), 8));
+  SIGMO_TRY(tmp_alloc(q, reinterpret_cast<void**>(&d_total), 8));
   int rc = cudaMemsetAsync(d_total, 0, 8, q->stream) == cudaSuccess ? SIGMO_OK : fail(SIGMO_ERR_CUDA, "memset failed");
   // the planes route takes any batch whose query graphs each fit an admission
   // tile (larger batches are admitted in groups); planes take 8 B per

@@ -202,6 +202,13 @@ int stage_end(Queue* q);
 // Stream-ordered device allocation on the queue's stream.
 int dev_alloc(Queue* q, void** p, size_t bytes);
 void dev_free(Queue* q, void* p);
+// Per-call temporaries (freed before the call returns): stream-ordered, from
+// a pool of their own per device that keeps its memory, so a call's buffers
+// are carved from blocks the previous calls freed even when the caller
+// creates and destroys graphs between calls (graph arrays come from the
+// device's default pool).  Inside a stream capture they come from the
+// default pool as graph memory nodes.  Free with dev_free.
+int tmp_alloc(Queue* q, void** p, size_t bytes);
 // Queue-owned scratch of at least `bytes` (contents undefined).
 int queue_scratch(Queue* q, size_t bytes, void** p);
 

@@ -182,7 +182,7 @@ int launch_gmcr_from_admit(Queue* q, const Graph* query, const Graph* data, cons
   if (G) cub::DeviceScan::InclusiveSum(nullptr, cub_bytes, static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
                                        static_cast<int>(G), q->stream);
   void* cub_tmp = nullptr;
-  SIGMO_TRY(dev_alloc(q, &cub_tmp, cub_bytes + 256));
+  SIGMO_TRY(tmp_alloc(q, &cub_tmp, cub_bytes + 256));
   int rc = SIGMO_OK;
   if (G && QG) {
     cudaError_t e = cub::DeviceScan::InclusiveSum(cub_tmp, cub_bytes, counts, m->offsets + 1, static_cast<int>(G), q->stream);
@@ -231,7 +231,7 @@ int launch_gmcr_from_ne(Queue* q, const Graph* query, const Graph* data, const u
   const uint64_t admit_words = static_cast<uint64_t>(QG) * GW;
   auto al = [](size_t x) { return (x + 255) & ~static_cast<size_t>(255); };
   void* buf = nullptr;
-  SIGMO_TRY(dev_alloc(q, &buf, al(admit_words * 4) + al(G * 4ull) + 256));
+  SIGMO_TRY(tmp_alloc(q, &buf, al(admit_words * 4) + al(G * 4ull) + 256));
   uint32_t* admit = static_cast<uint32_t*>(buf);
   uint32_t* counts = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + al(admit_words * 4));
   int rc = SIGMO_OK;
@@ -251,7 +251,7 @@ int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidate
   const uint32_t GW = (G + 31u) / 32u;
   const uint64_t Qn = query->total_nodes;
   void* ne = nullptr;
-  SIGMO_TRY(dev_alloc(q, &ne, 4ull * Qn * GW + 4));
+  SIGMO_TRY(tmp_alloc(q, &ne, 4ull * Qn * GW + 4));
   uint32_t* NE = static_cast<uint32_t*>(ne);
   int rc = SIGMO_OK;
   if (G && query->num_graphs && Qn) {

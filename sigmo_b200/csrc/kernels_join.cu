@@ -1520,7 +1520,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
   SIGMO_TRY(launch_query_order(const_cast<Graph*>(query)));
   const uint32_t skip = exact ? 0u : data->low_offset_graphs;
   void* buf = nullptr;
-  SIGMO_TRY(dev_alloc(q, &buf, 256 + 4ull * m->total));
+  SIGMO_TRY(tmp_alloc(q, &buf, 256 + 4ull * m->total));
   // [0] work cursor of the even chunks, [1] generic-join cursor, [2] overflow length, [3] odd chunks' cursor
   auto* ctr = static_cast<unsigned long long*>(buf);
   uint32_t* overflow = reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + 256);
@@ -1539,8 +1539,8 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
     two = m->total > chunk;
     const size_t mbytes = 8ull * kPhaseLevels * chunk + 16ull * chunk;
     void* mbuf[2] = {nullptr, nullptr};
-    rc = dev_alloc(q, &mbuf[0], mbytes);
-    if (!rc && two) rc = dev_alloc(q, &mbuf[1], mbytes);
+    rc = tmp_alloc(q, &mbuf[0], mbytes);
+    if (!rc && two) rc = tmp_alloc(q, &mbuf[1], mbytes);
     const cudaStream_t streams[2] = {q->stream, q->aux};
     if (!rc && two &&
         (cudaEventRecord(q->ev_aux_fork, q->stream) != cudaSuccess || cudaStreamWaitEvent(q->aux, q->ev_aux_fork, 0) != cudaSuccess))

@@ -384,7 +384,7 @@ __global__ void k_label_hist(const uint8_t* __restrict__ lab, uint64_t n, unsign
 int ensure_label_hist(Queue* q, Graph* g) {
   if (g->label_hist.size() == 256) return SIGMO_OK;
   void* buf = nullptr;
-  SIGMO_TRY(dev_alloc(q, &buf, 256 * 8));
+  SIGMO_TRY(tmp_alloc(q, &buf, 256 * 8));
   int rc = SIGMO_OK;
   if (cudaMemsetAsync(buf, 0, 256 * 8, q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "memset failed");
   if (!rc && g->total_nodes) {

@@ -288,7 +288,7 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
   if (!rc && QG) {
     void* buf = nullptr;
     const uint64_t total = w->m->total;
-    note(dev_alloc(q, &buf, 16ull * QG + 256));
+    note(tmp_alloc(q, &buf, 16ull * QG + 256));
     auto* d_matched = static_cast<unsigned long long*>(buf);
     auto* d_sum = d_matched + QG;
     if (!rc && cudaMemsetAsync(buf, 0, 16ull * QG, q->stream) != cudaSuccess) note(fail(SIGMO_ERR_CUDA, "memset failed"));
@@ -314,7 +314,7 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
       cub::DeviceScan::ExclusiveSum(nullptr, temp, static_cast<const uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
                                     static_cast<int>(std::min<uint64_t>(total, 0x7FFFFFFF)), q->stream);
       const uint64_t b_flag = (4 * total + 255) & ~255ull;
-      note(dev_alloc(q, &pbuf, 2 * b_flag + temp + 256));
+      note(tmp_alloc(q, &pbuf, 2 * b_flag + temp + 256));
       if (!rc) {
         auto* flag = static_cast<uint32_t*>(pbuf);
         auto* pos = reinterpret_cast<uint32_t*>(static_cast<char*>(pbuf) + b_flag);
@@ -331,7 +331,7 @@ void Server::run_batch(Worker* w, std::vector<Request*>& batch) {
         if (!rc && cudaStreamSynchronize(q->stream) != cudaSuccess) note(fail(SIGMO_ERR_CUDA, "synchronisation failed"));
         const uint64_t np = static_cast<uint64_t>(last[0]) + last[1];
         void* obuf = nullptr;
-        if (!rc) note(dev_alloc(q, &obuf, 16ull * np + 256));
+        if (!rc) note(tmp_alloc(q, &obuf, 16ull * np + 256));
         if (!rc) {
           auto* oq = static_cast<uint32_t*>(obuf);
           auto* og = oq + np;
@@ -552,14 +552,14 @@ int sigmo_server_create(int device, const sigmo_host_graphs* database, const sig
     if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) return cleanup(fail(SIGMO_ERR_CUDA, "cudaMemGetInfo failed"));
     s->so.memory_budget = freeb / 2;
   }
-  // Warm the device memory pool: one allocation of a quarter of the budget,
-  // freed at once.  The pool keeps the memory (its release threshold is
-  // unlimited), so the batches' stream-ordered allocations are carved from it
-  // instead of mapping new memory while requests wait.
+  // Warm the pool of per-call temporaries: one allocation of a quarter of the
+  // budget, freed at once.  The pool keeps the memory (its release threshold
+  // is unlimited), so the batches' stream-ordered temporaries are carved from
+  // it instead of mapping new memory while requests wait.
   {
     void* warm = nullptr;
     const uint64_t want = std::min<uint64_t>(s->so.memory_budget / 4, 32ull << 30);
-    if (want && dev_alloc(s->q0, &warm, want) == SIGMO_OK) {
+    if (want && tmp_alloc(s->q0, &warm, want) == SIGMO_OK) {
       dev_free(s->q0, warm);
       cudaStreamSynchronize(s->q0->stream);
     }
