@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <thread>
 #include <cstring>
 #include <vector>
 
@@ -39,6 +40,28 @@ void free_program(Queue* q, PlaneProgram* pp) {
   dev_free(q, pp->qsig_all);
   pp->qc_off = pp->qc = nullptr;
   *pp = PlaneProgram{};
+}
+
+// Threads for host loops over n items: one per 1,024 items, at most 8 and at
+// most the machine's hardware threads.
+unsigned host_threads(uint64_t n) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>({n / 1024, 8, hw})));
+}
+// f(part, begin, end) over `parts` contiguous ranges of [0, n), part 0 on the
+// calling thread; parts <= 1 (or `force_serial`) runs inline.
+template <class F>
+void parallel_ranges(uint64_t n, unsigned parts, F&& f, int force_serial = 0) {
+  if (parts <= 1 || force_serial) {
+    for (unsigned p = 0; p < parts; ++p) f(p, n * p / parts, n * (p + 1) / parts);
+    if (parts == 0) f(0, 0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(parts - 1);
+  for (unsigned p = 1; p < parts; ++p) th.emplace_back([&, p] { f(p, n * p / parts, n * (p + 1) / parts); });
+  f(0, 0, n / parts);
+  for (auto& t : th) t.join();
 }
 
 int upload(Queue* q, void** dst, const void* src, size_t bytes) {
@@ -79,23 +102,46 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   }
   SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));
 
+  // One pass over the signatures (vertex ranges in parallel): every vertex's
+  // program as raw codes (its label, then (r << 8 | l << 4 | c) for each
+  // non-zero counter in (r, l) order, rows of a fixed stride of 1 + 16 R
+  // entries), marking the labels and thresholds that occur.  Plane ids are
+  // assigned in label and (r, l, c) order, so raw codes sort like the plane
+  // ids they map to.
+  const uint32_t stride = 1 + 16 * R;
+  std::vector<uint16_t> vraw(static_cast<size_t>(Qn) * stride);
+  std::vector<uint32_t> vlen(Qn);
+  const unsigned nt = host_threads(Qn);
+  std::vector<std::vector<uint16_t>> thr_part(nt, std::vector<uint16_t>(static_cast<size_t>(R) * 16, 0));
+  std::vector<std::vector<uint8_t>> lab_part(nt, std::vector<uint8_t>(256, 0));
+  parallel_ranges(Qn, nt, [&](unsigned t, uint64_t v0, uint64_t v1) {
+    uint16_t* tm = thr_part[t].data();
+    uint8_t* lu = lab_part[t].data();
+    for (uint64_t v = v0; v < v1; ++v) {
+      uint16_t* row = vraw.data() + v * stride;
+      uint32_t n = 0;
+      lu[lab[v]] = 1;
+      row[n++] = lab[v];
+      for (uint32_t r = 0; r < R; ++r)
+        for (uint64_t sv = sig[static_cast<size_t>(r) * Qn + v]; sv;) {
+          const uint32_t l = static_cast<uint32_t>(__builtin_ctzll(sv)) >> 2, c = (sv >> (4 * l)) & 0xFu;
+          tm[r * 16 + l] |= static_cast<uint16_t>(1u << c);
+          row[n++] = static_cast<uint16_t>((r << 8) | (l << 4) | c);
+          sv &= ~(0xFull << (4 * l));
+        }
+      vlen[v] = n;
+    }
+  });
+  std::vector<uint8_t> label_used(256, 0);
+  std::vector<uint16_t> thr_mask(static_cast<size_t>(R) * 16, 0);  // [r][l]: bit c = count c occurs
+  for (unsigned t = 0; t < nt; ++t) {
+    for (size_t i = 0; i < thr_mask.size(); ++i) thr_mask[i] |= thr_part[t][i];
+    for (size_t i = 0; i < 256; ++i) label_used[i] |= lab_part[t][i];
+  }
   // planes: label values used by queries (ascending), then the thresholds
   // (r, l, c) that occur, in (r, l, c) order
-  std::vector<uint8_t> label_used(256, 0);
-  for (uint64_t v = 0; v < Qn; ++v) label_used[lab[v]] = 1;
-  std::vector<uint8_t> thr_used(static_cast<size_t>(R) * 16 * 16, 0);  // [r][l][c]
-  // non-zero counters only: bit 4l of the nibble mask is set when counter l is
-  auto for_counters = [](uint64_t sv, auto&& f) {
-    for (uint64_t nz = sig_nonzero_nibbles(sv); nz; nz &= nz - 1) {
-      const uint32_t l = static_cast<uint32_t>(__builtin_ctzll(nz)) >> 2;
-      f(l, static_cast<uint32_t>((sv >> (4 * l)) & 0xFu));
-    }
-  };
-  for (uint32_t r = 0; r < R; ++r)
-    for (uint64_t v = 0; v < Qn; ++v)
-      for_counters(sig[r * Qn + v], [&](uint32_t l, uint32_t c) { thr_used[(r * 16 + l) * 16 + c] = 1; });
   std::vector<uint32_t> spec;
-  std::vector<uint32_t> label_idx(256, 0), thr_idx(thr_used.size(), 0);
+  std::vector<uint32_t> label_idx(256, 0), thr_idx(static_cast<size_t>(R) * 256, 0);
   for (uint32_t l = 0; l < 256; ++l)
     if (label_used[l]) {
       label_idx[l] = static_cast<uint32_t>(spec.size());
@@ -105,55 +151,57 @@ int build_plane_program(Queue* q, Graph* query, uint32_t R) {
   for (uint32_t r = 0; r < R; ++r)
     for (uint32_t l = 0; l < 16; ++l)
       for (uint32_t c = 1; c < 16; ++c)
-        if (thr_used[(r * 16 + l) * 16 + c]) {
-          thr_idx[(r * 16 + l) * 16 + c] = static_cast<uint32_t>(spec.size());
+        if ((thr_mask[r * 16 + l] >> c) & 1u) {
+          thr_idx[(r << 8) | (l << 4) | c] = static_cast<uint32_t>(spec.size());
           spec.push_back((r << 16) | (l << 8) | c);
         }
   if (spec.size() >= 65535) return fail(SIGMO_ERR_DOMAIN, "query batch needs %zu candidate planes (limit 65535)", spec.size());
 
-  // classes: distinct (label, sig_1..sig_R); program = label plane, then the
-  // thresholds in (r, l) order; classes numbered in lexicographic program
-  // order (one sort of the vertices by program).
-  std::vector<uint32_t> voff(Qn + 1, 0);
-  std::vector<uint16_t> vprog;
-  vprog.reserve(Qn * 8);
-  for (uint64_t v = 0; v < Qn; ++v) {
-    vprog.push_back(static_cast<uint16_t>(label_idx[lab[v]]));
-    for (uint32_t r = 0; r < R; ++r)
-      for_counters(sig[r * Qn + v],
-                   [&](uint32_t l, uint32_t c) { vprog.push_back(static_cast<uint16_t>(thr_idx[(r * 16 + l) * 16 + c])); });
-    voff[v + 1] = static_cast<uint32_t>(vprog.size());
-  }
-  // sort key: the first four plane ids packed high to low (missing ones 0:
-  // only position 0, the label plane, can hold id 0, so a shorter program
-  // still sorts first); ties fall back to the full comparison
-  std::vector<uint64_t> pkey(Qn);
-  for (uint64_t v = 0; v < Qn; ++v) {
-    uint64_t k = 0;
-    for (uint32_t i = 0; i < 4; ++i) k = (k << 16) | (voff[v] + i < voff[v + 1] ? vprog[voff[v] + i] : 0u);
-    pkey[v] = k;
-  }
-  auto prog_less = [&](uint32_t a, uint32_t b2) {
-    if (pkey[a] != pkey[b2]) return pkey[a] < pkey[b2];
-    return std::lexicographical_compare(vprog.begin() + voff[a], vprog.begin() + voff[a + 1], vprog.begin() + voff[b2],
-                                        vprog.begin() + voff[b2 + 1]);
+  // classes: distinct (label, sig_1..sig_R), numbered in lexicographic program
+  // order: the vertices sorted by (the first four raw codes packed high to low,
+  // a shorter program's missing codes 0 so it sorts first; ties: the full
+  // comparison), in parallel ranges merged pairwise
+  struct Key {
+    uint64_t k;
+    uint32_t v;
   };
-  auto prog_equal = [&](uint32_t a, uint32_t b2) {
-    return voff[a + 1] - voff[a] == voff[b2 + 1] - voff[b2] &&
-           std::equal(vprog.begin() + voff[a], vprog.begin() + voff[a + 1], vprog.begin() + voff[b2]);
+  std::vector<Key> keys(Qn);
+  auto row_of = [&](uint32_t v) { return vraw.data() + static_cast<size_t>(v) * stride; };
+  auto key_less = [&](const Key& x, const Key& y) {
+    if (x.k != y.k) return x.k < y.k;
+    return std::lexicographical_compare(row_of(x.v), row_of(x.v) + vlen[x.v], row_of(y.v), row_of(y.v) + vlen[y.v]);
   };
-  std::vector<uint32_t> by_prog(Qn);
-  for (uint64_t v = 0; v < Qn; ++v) by_prog[v] = static_cast<uint32_t>(v);
-  std::sort(by_prog.begin(), by_prog.end(), prog_less);
+  std::vector<uint64_t> cut(nt + 1);
+  for (unsigned t = 0; t <= nt; ++t) cut[t] = Qn * t / nt;
+  parallel_ranges(Qn, nt, [&](unsigned, uint64_t v0, uint64_t v1) {
+    for (uint64_t v = v0; v < v1; ++v) {
+      const uint16_t* row = row_of(static_cast<uint32_t>(v));
+      uint64_t k = 0;
+      for (uint32_t i = 0; i < 4; ++i) k = (k << 16) | (i < vlen[v] ? row[i] : 0u);
+      keys[v] = Key{k, static_cast<uint32_t>(v)};
+    }
+    std::sort(keys.begin() + v0, keys.begin() + v1, key_less);
+  });
+  for (unsigned w = 1; w < nt; w *= 2)  // pairwise merges of the sorted ranges
+    parallel_ranges(nt, (nt + 2 * w - 1) / (2 * w), [&](unsigned, uint64_t g0, uint64_t g1) {
+      for (uint64_t g = g0; g < g1; ++g) {
+        const uint64_t a = 2 * w * g, m = std::min<uint64_t>(a + w, nt), b = std::min<uint64_t>(a + 2 * w, nt);
+        if (m < b) std::inplace_merge(keys.begin() + cut[a], keys.begin() + cut[m], keys.begin() + cut[b], key_less);
+      }
+    }, 1);
   std::vector<uint32_t> cls(Qn), prog_off{0};
   std::vector<uint16_t> prog;
+  prog.reserve(static_cast<size_t>(Qn) * 8);
   uint32_t max_len = 0;
   for (uint64_t i = 0; i < Qn; ++i) {
-    const uint32_t v = by_prog[i];
-    if (i == 0 || !prog_equal(by_prog[i - 1], v)) {
-      prog.insert(prog.end(), vprog.begin() + voff[v], vprog.begin() + voff[v + 1]);
+    const uint32_t v = keys[i].v;
+    if (i == 0 || keys[i - 1].k != keys[i].k || vlen[keys[i - 1].v] != vlen[v] ||
+        !std::equal(row_of(v), row_of(v) + vlen[v], row_of(keys[i - 1].v))) {
+      const uint16_t* row = row_of(v);
+      prog.push_back(static_cast<uint16_t>(label_idx[row[0]]));
+      for (uint32_t j = 1; j < vlen[v]; ++j) prog.push_back(static_cast<uint16_t>(thr_idx[row[j]]));
       prog_off.push_back(static_cast<uint32_t>(prog.size()));
-      max_len = std::max<uint32_t>(max_len, voff[v + 1] - voff[v]);
+      max_len = std::max<uint32_t>(max_len, vlen[v]);
     }
     cls[v] = static_cast<uint32_t>(prog_off.size() - 2);
   }
@@ -321,18 +369,26 @@ int order_classes(Queue* q, Graph* query, Graph* data) {
   const uint32_t QG = query->num_graphs;
   uint64_t all = 0;
   for (uint64_t x : data->label_hist) all += x;
-  std::vector<uint32_t> off{0}, list, tmp;
+  // query graphs in parallel ranges, each query's list on its own, then
+  // concatenated in query order
+  std::vector<std::vector<uint32_t>> per(QG);
+  auto key = [&](uint32_t c) {
+    const uint32_t lab = pp.h_spec[pp.h_prog[pp.h_prog_off[c]]] & 0xFFu;
+    const uint64_t freq = lab == kWildcard ? all : data->label_hist[lab];
+    return std::make_tuple(freq, 0u - (pp.h_prog_off[c + 1] - pp.h_prog_off[c]), c);
+  };
+  parallel_ranges(QG, host_threads(query->total_nodes), [&](unsigned, uint64_t q0, uint64_t q1) {
+    for (uint64_t qg = q0; qg < q1; ++qg) {
+      std::vector<uint32_t>& tmp = per[qg];
+      tmp.assign(pp.h_cls.begin() + pp.h_qgoff[qg], pp.h_cls.begin() + pp.h_qgoff[qg + 1]);
+      std::sort(tmp.begin(), tmp.end());
+      tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+      std::sort(tmp.begin(), tmp.end(), [&](uint32_t a, uint32_t b) { return key(a) < key(b); });
+    }
+  });
+  std::vector<uint32_t> off{0}, list;
   for (uint32_t qg = 0; qg < QG; ++qg) {
-    tmp.assign(pp.h_cls.begin() + pp.h_qgoff[qg], pp.h_cls.begin() + pp.h_qgoff[qg + 1]);
-    std::sort(tmp.begin(), tmp.end());
-    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-    auto key = [&](uint32_t c) {
-      const uint32_t lab = pp.h_spec[pp.h_prog[pp.h_prog_off[c]]] & 0xFFu;
-      const uint64_t freq = lab == kWildcard ? all : data->label_hist[lab];
-      return std::make_tuple(freq, 0u - (pp.h_prog_off[c + 1] - pp.h_prog_off[c]), c);
-    };
-    std::sort(tmp.begin(), tmp.end(), [&](uint32_t a, uint32_t b) { return key(a) < key(b); });
-    list.insert(list.end(), tmp.begin(), tmp.end());
+    list.insert(list.end(), per[qg].begin(), per[qg].end());
     off.push_back(static_cast<uint32_t>(list.size()));
   }
   dev_free(q, pp.qc_off);
@@ -644,6 +700,24 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   Events ev;
   for (auto& e : ev.e) SIGMO_CUDA_TRY(cudaEventCreate(&e));
   SIGMO_CUDA_TRY(cudaEventRecord(ev.e[0], q->stream));
+  // the data graph's signatures do not depend on the query batch: launched
+  // first, they run while the host builds the query batch's plane program
+  BatchedRun prun = run;
+  uint64_t* dsig_tmp = nullptr;
+  if (!run.dsig && !run.capture && R && data->total_nodes) {
+    SIGMO_TRY(tmp_alloc(q, reinterpret_cast<void**>(&dsig_tmp), 8ull * R * data->total_nodes));
+    const int src = launch_sig_all(q, data, R, dsig_tmp);
+    if (src) {
+      dev_free(q, dsig_tmp);
+      return src;
+    }
+    prun.dsig = dsig_tmp;
+  }
+  struct FreeTmp {
+    Queue* q;
+    uint64_t* p;
+    ~FreeTmp() { dev_free(q, p); }
+  } free_dsig{q, dsig_tmp};
   SIGMO_TRY(build_plane_program(q, query, R));
   uint64_t* d_total = nullptr;
   SIGMO_TRY(tmp_alloc(q, reinterpret_cast<void**>(&d_total), 8));
@@ -664,10 +738,10 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
     if (bitset_route) {
       sigmo_candidates_t cc = static_cast<sigmo_candidates_t>(c);
       if (!cc) rc = sigmo_candidates_create(static_cast<sigmo_queue_t>(q), query->total_nodes, data->total_nodes, &cc);
-      if (!rc) rc = batched_bitset(q, query, data, R, find_first, cc, m, d_total, ev, run);
+      if (!rc) rc = batched_bitset(q, query, data, R, find_first, cc, m, d_total, ev, prun);
       if (cc != c) sigmo_candidates_destroy(cc);
     } else {
-      rc = batched_planes(q, query, data, R, find_first, m, d_total, ev, run);
+      rc = batched_planes(q, query, data, R, find_first, m, d_total, ev, prun);
     }
   }
   if (!rc && cudaEventRecord(ev.e[4], q->stream) != cudaSuccess) rc = fail(SIGMO_ERR_CUDA, "event record failed");
