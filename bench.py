@@ -726,8 +726,11 @@ def run_sigmo(args, rank, world, local):
 # ---- the reference arm ------------------------------------------------------------------
 def run_reference(args, rank, world, local):
     """The reference's algorithm on the host cores: the oracle (its CPU
-    restatement; the SYCL reference cannot be compiled here) on the same
-    workload and config as the sigmo arm.  Inputs come from the host-only
+    restatement, REF_PTX semantics, -O3 and OpenMP) on the same workload and
+    config as the sigmo arm.  No SYCL compiler is installed; the reference's
+    own source runs on the host only through the SYCL stand-in under
+    oracle/ (one work-group at a time, -O0), which computes the REF_X86
+    semantics and serves as the oracle's checker, not as a timed baseline.  Inputs come from the host-only
     workload library (oracle/libsigmo_workload.so, the same seeded
     generator), so this arm never maps the product's CUDA library.  Each step
     runs the full pipeline on the next contiguous slice of the workload's
@@ -772,8 +775,9 @@ def run_reference(args, rank, world, local):
     v = pairs / sum(times)
     sample = (f"{args.steps} timed steps, each the full pipeline on the next {per_step} molecules of the workload (ids "
               f"re-based to 0) x all {q.num_graphs} queries ({'find-first' if ff else 'find-all'}, {wl['R']} "
-              f"iterations); the SYCL reference cannot be compiled here (no SYCL compiler), so its CPU restatement "
-              f"runs on all host threads")
+              f"iterations); no SYCL compiler is installed (the reference's own source builds for the host only "
+              f"through a one-work-group-at-a-time SYCL stand-in at -O0 with REF_X86 semantics, used as the "
+              f"oracle's checker), so its CPU restatement runs, on all host threads")
     line = {
         "impl": "reference",
         "metric": METRIC,
