@@ -875,6 +875,10 @@ __global__ void __launch_bounds__(128) k_join_fast(
 constexpr uint32_t kPhaseLevels = 16;
 constexpr uint32_t kPhaseThreads = 256;
 
+// Work layout: a warp takes 32 consecutive slots per round, one lane per slot
+// for the slot's metadata and setup record, then the round's sum of query
+// sizes (slot, level) items with every lane busy; an item finds its slot by a
+// binary search over the lanes' exclusive prefix sums (warp shuffles).
 __global__ void __launch_bounds__(256) k_pair_masks(
     const uint64_t* __restrict__ planes, uint32_t K, uint32_t AW, const uint32_t* __restrict__ prog_off,
     const uint16_t* __restrict__ prog,
@@ -883,34 +887,64 @@ __global__ void __launch_bounds__(256) k_pair_masks(
     const uint32_t* __restrict__ indices, const uint32_t* __restrict__ pair_graph, uint64_t slot0, uint64_t count,
     uint64_t* __restrict__ masks, uint4* __restrict__ rec, uint32_t skip_below, uint32_t* __restrict__ overflow,
     unsigned long long* __restrict__ overflow_len, uint64_t* __restrict__ counts) {
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count * kPhaseLevels; i += stride) {
-    const uint64_t local = i / kPhaseLevels;  // slot within the chunk, then level (fastest)
-    const uint32_t j = static_cast<uint32_t>(i % kPhaseLevels);
-    const uint64_t slot = slot0 + local;
-    const uint32_t qg = indices[slot];
-    const uint32_t qoff = qgoff[qg], n = qgoff[qg + 1] - qoff;
-    if (j >= n) continue;
-    const uint32_t g = pair_graph[slot];
-    const bool ident = !(qsym[qg] && dsym[g]);
-    // queries over kPhaseLevels vertices and molecules over 64 atoms (a
-    // vertex set wider than one word) go to the generic kernel
-    const bool generic = n > kPhaseLevels || dgoff[g + 1] - dgoff[g] > 64u;
-    if (j == 0) {  // the pair's setup record: first data vertex, query size | flags, query offset, data graph
-      rec[local] = make_uint4(dgoff[g], n | (ident ? 0x100u : 0u) | (generic ? 0x200u : 0u), qoff, g);
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t s0 = warp * 32; s0 < count; s0 += nwarps * 32) {
+    const uint64_t local = s0 + lane;
+    uint32_t n = 0, qoff = 0, g = 0, items = 0;
+    bool ident = true;
+    if (local < count) {
+      const uint64_t slot = slot0 + local;
+      const uint32_t qg = indices[slot];
+      qoff = qgoff[qg];
+      n = qgoff[qg + 1] - qoff;
+      g = pair_graph[slot];
+      ident = !(qsym[qg] && dsym[g]);
+      const uint32_t ds = dgoff[g];
+      // queries over kPhaseLevels vertices and molecules over 64 atoms (a
+      // vertex set wider than one word) go to the generic kernel
+      const bool generic = n > kPhaseLevels || dgoff[g + 1] - ds > 64u;
+      // the pair's setup record: first data vertex, query size | flags, query offset, data graph
+      rec[local] = make_uint4(ds, n | (ident ? 0x100u : 0u) | (generic ? 0x200u : 0u), qoff, g);
       if (generic && g >= skip_below) {  // joined by the generic kernel, which accumulates into counts
         overflow[atomicAdd(overflow_len, 1ull)] = static_cast<uint32_t>(slot);
         counts[slot] = 0;
       }
+      items = generic ? 0u : n;
     }
-    if (generic) continue;
-    const uint32_t c = cls[qoff + (ident ? j : qorder[qoff + j])];
-    // word 0 of each plane: the graph's vertex set fits one word
-    const uint64_t* base = planes + static_cast<uint64_t>(g >> 5) * K * AW * 32 + (g & 31u);
-    uint64_t m = ~0ull;
-    const uint32_t e1 = prog_off[c + 1];
-    for (uint32_t e = prog_off[c]; e < e1; ++e) m &= base[static_cast<uint64_t>(prog[e]) * AW * 32];
-    masks[local * kPhaseLevels + j] = m;
+    uint32_t incl = items;
+#pragma unroll
+    for (unsigned o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const uint32_t excl = incl - items;
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t it = base + lane;
+      // owner: the last lane whose exclusive prefix is <= it
+      uint32_t pos = 0;
+#pragma unroll
+      for (uint32_t step = 16; step; step >>= 1) {
+        const uint32_t cand = pos + step;
+        const uint32_t e = __shfl_sync(0xFFFFFFFFu, excl, cand & 31u);
+        if (cand < 32u && e <= it) pos = cand;
+      }
+      const uint32_t o_excl = __shfl_sync(0xFFFFFFFFu, excl, pos);
+      const uint32_t o_qoff = __shfl_sync(0xFFFFFFFFu, qoff, pos);
+      const uint32_t o_g = __shfl_sync(0xFFFFFFFFu, g, pos);
+      const bool o_ident = __shfl_sync(0xFFFFFFFFu, static_cast<unsigned>(ident), pos) != 0u;
+      if (it >= total) continue;
+      const uint32_t j = it - o_excl;
+      const uint32_t c = cls[o_qoff + (o_ident ? j : qorder[o_qoff + j])];
+      // word 0 of each plane: the graph's vertex set fits one word
+      const uint64_t* pb = planes + static_cast<uint64_t>(o_g >> 5) * K * AW * 32 + (o_g & 31u);
+      uint64_t m = ~0ull;
+      const uint32_t e1 = prog_off[c + 1];
+      for (uint32_t e = prog_off[c]; e < e1; ++e) m &= pb[static_cast<uint64_t>(prog[e]) * AW * 32];
+      masks[(s0 + pos) * kPhaseLevels + j] = m;
+    }
   }
 }
 
@@ -1574,7 +1608,7 @@ int launch_join_fast_planes(Queue* q, const Graph* query, const Graph* data, con
       auto* masks = static_cast<uint64_t*>(mbuf[c & 1]);
       auto* recs = reinterpret_cast<uint4*>(masks + kPhaseLevels * chunk);
       unsigned long long* cursor = ctr + ((c & 1) ? 3 : 0);
-      k_pair_masks<<<grid_for(cnt * kPhaseLevels, 256, 148u * 32u), 256, 0, st>>>(
+      k_pair_masks<<<grid_for(cnt, 256, 148u * 16u), 256, 0, st>>>(
           planes, planes_rows, data->adj_words, pp.prog_off, prog, pp.cls, query->graph_offsets, query->qorder, query->sym,
           data->graph_offsets, data->sym, m->indices, m->pair_graph, slot0, cnt, masks, recs, skip, overflow, ctr + 2,
           m->counts);
