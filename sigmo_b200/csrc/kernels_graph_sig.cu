@@ -192,16 +192,112 @@ __global__ void k_sig_refine_exact(uint64_t N, const uint32_t* __restrict__ goff
 // All refinement iterations 1..R at once (batched form): starting from empty
 // reachables, iteration r's sphere is exactly BFS level r, so one BFS to
 // depth R emits every iteration's signature.  sig_all is [R][N].
+//
+// Each CTA's graphs are staged on chip.  A CTA takes 256 consecutive
+// vertices; they belong to a run of whole graphs whose adjacency rows
+// [row_lo, row_hi) (at most 256 + 128 * AW rows for graphs of up to 64 * AW
+// vertices) arrive in shared memory by one bulk asynchronous copy (the TMA
+// engine, cp.async.bulk, completion counted on an mbarrier), and whose labels
+// arrive by plain loads meanwhile; every vertex's BFS then reads shared memory
+// only.  The copy starts on a 16-byte boundary of the adjacency array, is a
+// multiple of 16 bytes and ends inside the array (a last 8-byte row past the
+// final 16-byte boundary is loaded by a thread).  A range whose graphs do not
+// fit (wide graphs) reads global memory instead.  The mbarrier
+// wait is bounded; past the bound the range is computed from global memory
+// (results are the same either way) and the CTA stops staging.
+constexpr uint32_t kSigRange = 256;
+constexpr uint32_t kSigSpinLimit = 1u << 22;
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a), "r"(bytes) : "memory");
+}
+// Bulk global -> shared copy of `bytes` (multiple of 16; both addresses
+// 16-byte aligned), its completion counted on `bar`.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d), "l"(src),
+               "r"(bytes), "r"(b)
+               : "memory");
+}
+// Waits (bounded) for phase `parity` of `bar` to complete; false if it did not.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  for (uint32_t i = 0; i < kSigSpinLimit; ++i) {
+    uint32_t done = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 template <int AW, bool EXACT>
-__global__ void k_sig_all(uint64_t N, const uint32_t* __restrict__ goff, const uint32_t* __restrict__ node_graph,
-                          const uint64_t* __restrict__ adj, const uint32_t* __restrict__ roff,
-                          const uint32_t* __restrict__ col, const uint8_t* __restrict__ lab, uint32_t Rn,
-                          uint64_t* __restrict__ sig_all) {
-  for (uint64_t vv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; vv < N; vv += (uint64_t)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(kSigRange) k_sig_all_staged(uint64_t N, const uint32_t* __restrict__ goff,
+                                                              const uint32_t* __restrict__ node_graph,
+                                                              const uint64_t* __restrict__ adj,
+                                                              const uint32_t* __restrict__ roff,
+                                                              const uint32_t* __restrict__ col,
+                                                              const uint8_t* __restrict__ lab, uint32_t Rn,
+                                                              uint64_t* __restrict__ sig_all) {
+  constexpr uint32_t kCap = kSigRange + 128u * AW;         // rows of one range's graphs, at most
+  __shared__ __align__(16) uint64_t s_rows[kCap * AW + 2];  // + 16 bytes: the copy may start one row early
+  __shared__ uint8_t s_lab[kCap];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ int s_ok;  // the CTA still stages (no wait has run out)
+  const uint64_t adj_bytes = N * AW * 8ull;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    s_ok = 1;
+  }
+  __syncthreads();
+  uint32_t parity = 0;
+  for (uint64_t v0 = static_cast<uint64_t>(blockIdx.x) * kSigRange; v0 < N; v0 += static_cast<uint64_t>(gridDim.x) * kSigRange) {
+    const uint64_t v1 = v0 + kSigRange < N ? v0 + kSigRange : N;
+    const uint32_t row_lo = goff[node_graph[v0]], row_hi = goff[node_graph[v1 - 1] + 1];
+    const bool stage = s_ok && row_hi - row_lo <= kCap;  // the same for every thread
+    __syncthreads();  // the previous range's rows and labels are no longer read
+    uint32_t extra = 0;  // words copied before row_lo (the copy starts on a 16-byte boundary)
+    if (stage) {
+      const uint64_t b_lo = static_cast<uint64_t>(row_lo) * AW * 8, b_hi = static_cast<uint64_t>(row_hi) * AW * 8;
+      const uint64_t a_lo = b_lo & ~15ull;
+      const uint64_t a_hi = (b_hi + 15) & ~15ull;
+      const uint64_t c_hi = a_hi <= adj_bytes ? a_hi : (b_hi & ~15ull);  // the copy ends inside the array
+      extra = static_cast<uint32_t>((b_lo - a_lo) / 8);
+      if (threadIdx.x == 0) {
+        if (c_hi > a_lo) {
+          mbar_expect_tx(&s_bar, static_cast<uint32_t>(c_hi - a_lo));
+          bulk_copy_g2s(s_rows, reinterpret_cast<const char*>(adj) + a_lo, static_cast<uint32_t>(c_hi - a_lo), &s_bar);
+        } else {
+          mbar_expect_tx(&s_bar, 0);  // completes the phase with nothing in flight
+        }
+      }
+      if (threadIdx.x == 32 && c_hi < b_hi)  // the last 8-byte row past the final 16-byte boundary
+        s_rows[(c_hi - a_lo) / 8] = adj[(c_hi) / 8];
+      for (uint32_t i = threadIdx.x; i < row_hi - row_lo; i += blockDim.x) s_lab[i] = lab[row_lo + i];
+      if (!mbar_wait(&s_bar, parity)) s_ok = 0;
+      parity ^= 1u;
+    }
+    __syncthreads();  // labels and the tail row are in; s_ok is settled
+    const bool use_smem = stage && s_ok;
+    const uint64_t vv = v0 + threadIdx.x;
+    if (vv >= v1) continue;
     const uint32_t v = static_cast<uint32_t>(vv);
     const uint32_t prev = goff[node_graph[v]];
     const uint32_t n = goff[node_graph[v] + 1] - prev;
     const uint32_t lv = v - prev;
+    // rows and labels of this vertex's graph: shared memory or global memory
+    const uint64_t* grow = use_smem ? s_rows + extra + static_cast<uint64_t>(prev - row_lo) * AW : adj + static_cast<uint64_t>(prev) * AW;
+    const uint8_t* glab = use_smem ? s_lab + (prev - row_lo) : lab + prev;
     uint64_t F[AW], R[AW];
     const bool wide = !EXACT && n > 256u;
 #pragma unroll
@@ -225,7 +321,7 @@ __global__ void k_sig_all(uint64_t N, const uint32_t* __restrict__ goff, const u
           while (m) {
             const uint32_t b = __ffsll(static_cast<long long>(m)) - 1 + 64u * w;
             m &= m - 1;
-            const uint64_t* row = adj + static_cast<uint64_t>(prev + b) * AW;
+            const uint64_t* row = grow + static_cast<uint64_t>(b) * AW;
 #pragma unroll
             for (int k = 0; k < AW; ++k) nx[k] |= row[k];
           }
@@ -239,7 +335,7 @@ __global__ void k_sig_all(uint64_t N, const uint32_t* __restrict__ goff, const u
             const uint32_t u = prev + b;
             for (uint32_t i = roff[u]; i < roff[u + 1]; ++i) nx[0] |= refbit(col[i] - prev, 0);
           } else {
-            nx[0] |= adj[static_cast<uint64_t>(prev + b) * AW];
+            nx[0] |= grow[static_cast<uint64_t>(b) * AW];
           }
         }
       }
@@ -253,13 +349,17 @@ __global__ void k_sig_all(uint64_t N, const uint32_t* __restrict__ goff, const u
         while (sphere) {
           const uint32_t b = __ffsll(static_cast<long long>(sphere)) - 1;
           sphere &= sphere - 1;
-          s = sig_inc(s, lab[prev + 64u * k + b]);
+          s = sig_inc(s, glab[64u * k + b]);
         }
         if (!EXACT) break;
       }
       sig_all[static_cast<uint64_t>(r) * N + v] = s;
     }
   }
+  // a copy whose wait ran out may still be in flight: wait again (bounded)
+  // before the CTA's shared memory is released
+  __syncthreads();
+  if (!s_ok) mbar_wait(&s_bar, parity ^ 1u);
 }
 
 // Matching order per query graph (batched join): start at the vertex of
@@ -422,16 +522,16 @@ int launch_sig_all(Queue* q, const Graph* g, uint32_t R, uint64_t* sig_all) {
     if (g->max_nodes > 64u * kMaxAdjWords)
       return fail(SIGMO_ERR_DOMAIN, "exact profile supports graphs of at most %u vertices (largest: %u)", 64u * kMaxAdjWords, g->max_nodes);
     switch (g->adj_words) {
-      case 1: k_sig_all<1, true><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
-      case 2: k_sig_all<2, true><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
-      default: k_sig_all<4, true><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+      case 1: k_sig_all_staged<1, true><<<grid, kSigRange, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+      case 2: k_sig_all_staged<2, true><<<grid, kSigRange, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+      default: k_sig_all_staged<4, true><<<grid, kSigRange, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
     }
     return check_launch(q, "k_sig_all<exact>");
   }
   switch (g->adj_words) {
-    case 1: k_sig_all<1, false><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
-    case 2: k_sig_all<2, false><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
-    default: k_sig_all<4, false><<<grid, 256, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+    case 1: k_sig_all_staged<1, false><<<grid, kSigRange, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+    case 2: k_sig_all_staged<2, false><<<grid, kSigRange, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
+    default: k_sig_all_staged<4, false><<<grid, kSigRange, 0, q->stream>>>(g->total_nodes, g->graph_offsets, g->node_graph, g->adj, g->row_offsets, g->column_indices, g->node_labels, R, sig_all); break;
   }
   return check_launch(q, "k_sig_all<ptx>");
 }
