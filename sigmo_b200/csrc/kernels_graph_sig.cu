@@ -281,8 +281,11 @@ __global__ void __launch_bounds__(kSigRange) k_sig_all_staged(uint64_t N, const 
           mbar_expect_tx(&s_bar, 0);  // completes the phase with nothing in flight
         }
       }
-      if (threadIdx.x == 32 && c_hi < b_hi)  // the last 8-byte row past the final 16-byte boundary
+      if (threadIdx.x == 32 && c_hi < b_hi) {  // the last 8-byte row past the final 16-byte boundary
         s_rows[(c_hi - a_lo) / 8] = adj[(c_hi) / 8];
+        // order this generic store before any later bulk copy into the buffer
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      }
       for (uint32_t i = threadIdx.x; i < row_hi - row_lo; i += blockDim.x) s_lab[i] = lab[row_lo + i];
       if (!mbar_wait(&s_bar, parity)) s_ok = 0;
       parity ^= 1u;
