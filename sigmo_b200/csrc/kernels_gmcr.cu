@@ -17,71 +17,181 @@
 #include <algorithm>
 #include <mutex>
 
+#include "bulk.cuh"
 #include "internal.hpp"
 
 namespace sigmo_b200 {
 namespace {
 
-constexpr unsigned kNeRowsPerBlock = 64;
-constexpr unsigned kNeBatch = 8;  // rows whose words are loaded together
+// Non-empty pass: NE[j][g/32] bit g%32 = query vertex j has a range-masked
+// candidate in data graph g.  A CTA owns 256 consecutive data graphs (8 NE
+// words, lane = data graph) and a run of kNeRowsPerCta bitset rows.  The
+// words its graphs span in a row, [ws, we) rounded out to 16-byte
+// boundaries, arrive in shared memory by bulk asynchronous copies (one per
+// row, issued by the lanes of warp 0) into a ring of kNeStages stages whose
+// completion is counted on one mbarrier per stage; each warp then reads its
+// graphs' 1-3 words per row from shared memory, ANDs them with the graph's
+// range masks (computed once: only a graph's first and last words are
+// partial, candidates.hpp:91-99) and votes the row's NE word.  So DRAM sees
+// every bitset byte once in 16-byte-aligned bursts, and the per-row work is a
+// few shared-memory loads, logic ops, a vote and a store per warp.  A CTA
+// whose span exceeds one stage reads global memory instead (same results).
+// Waits are bounded: a thread whose wait runs out reads that chunk from
+// global memory, and warp 0 stops refilling a stage whose phase it did not
+// see complete (it waits for it again, bounded, before the CTA exits).
+constexpr uint32_t kNeThreads = 256;
+constexpr uint32_t kNeStages = 2;
+constexpr uint32_t kNeStageWords = 6144;  // 24 KiB per stage (4 CTAs per SM)
+constexpr uint32_t kNeRowsPerCta = 512;
+constexpr uint32_t kNeSleepNs = 20000;  // longest suspension per poll of a stage's mbarrier
+constexpr uint32_t kNePolls = 1u << 16;  // polls before a wait gives up (about a second at most)
+constexpr uint32_t kNePadWords = 4;       // slack for the fixed three-word reads of the last row
+constexpr size_t kNeSmemBytes = sizeof(uint32_t) * (kNeStages * kNeStageWords + kNePadWords);
 
-// Lane = data graph, warp = 32 consecutive graphs (their words are
-// contiguous, so a warp's loads for one row cover ~35 consecutive words).
-// kNeBatch rows are read per pass over the graph's words so that many loads
-// are in flight per lane.
-__global__ void k_gmcr_ne(const uint32_t* __restrict__ bits, uint64_t Wp, uint64_t Qn, const uint32_t* __restrict__ dgoff,
-                          uint32_t G, uint32_t GW, int prof, uint32_t* __restrict__ NE) {
-  const unsigned lane = threadIdx.x & 31u;
-  const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (gw >= GW) return;
-  const uint32_t g = gw * 32u + lane;
-  uint32_t s = 0, e = 0, i0 = 0, i1 = 0;
+struct NeLane {
+  uint32_t i0, nw;      // the graph's first word and word count (0: empty or past the last graph)
+  uint32_t mf, ml;      // range masks of its first and last words
+  uint32_t m0, m1, m2;  // masks of words 0..2 (nw <= 3)
+  uint32_t o1, o2;      // word offsets of words 1 and 2, clamped to the graph's words
+};
+
+// The NE bit of one row for a lane, from the row's words starting at `row`
+// (word i0 of the graph at row[0]).
+__device__ __forceinline__ bool ne_any_few(const uint32_t* row, const NeLane& L) {
+  return ((row[0] & L.m0) | (row[L.o1] & L.m1) | (row[L.o2] & L.m2)) != 0u;
+}
+__device__ __forceinline__ bool ne_any_wide(const uint32_t* row, const NeLane& L) {
+  uint32_t acc = 0;
+  for (uint32_t k = 0; k < L.nw; ++k) acc |= row[k] & (k == 0 ? L.mf : (k + 1 == L.nw ? L.ml : 0xFFFFFFFFu));
+  return acc != 0u;
+}
+
+// Warp 0 of k_gmcr_ne: the bulk copies of chunk c (RS rows of SW words from
+// row j0 + c * RS on, word ws on) into stage c % kNeStages.
+__device__ __forceinline__ void ne_issue(uint32_t c, uint32_t lane, uint32_t RS, uint32_t SW, uint32_t nrows, uint64_t j0,
+                                         uint32_t ws, uint64_t Wp, const uint32_t* __restrict__ bits, uint32_t* s_stage,
+                                         uint64_t* s_bar, uint32_t* s_live) {
+  const uint32_t st = c % kNeStages;
+  const uint32_t r0 = c * RS, nr = nrows - r0 < RS ? nrows - r0 : RS;
+  if (lane == 0) {
+    mbar_expect_tx(&s_bar[st], nr * SW * 4u);
+    s_live[st] = 1u;
+  }
+  __syncwarp();
+  if (lane < nr)
+    bulk_copy_g2s(s_stage + st * kNeStageWords + lane * SW, bits + (j0 + r0 + lane) * Wp + ws, SW * 4u, &s_bar[st]);
+}
+
+__global__ void __launch_bounds__(kNeThreads, 4) k_gmcr_ne(const uint32_t* __restrict__ bits, uint64_t Wp, uint64_t Qn,
+                                                        const uint32_t* __restrict__ dgoff, uint32_t G, uint32_t GW, int prof,
+                                                        uint32_t* __restrict__ NE) {
+  extern __shared__ __align__(128) uint32_t s_stage[];  // kNeStages x kNeStageWords, then kNePadWords
+  __shared__ __align__(8) uint64_t s_bar[kNeStages];
+  __shared__ uint32_t s_live[kNeStages];  // stage holds (or receives) the chunk its next reader expects
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t g_lo = blockIdx.x * kNeThreads;
+  const uint32_t g = g_lo + threadIdx.x;
+  const uint32_t gw = g_lo / 32u + warp;
+  NeLane L{};
   if (g < G) {
-    s = dgoff[g];
-    e = dgoff[g + 1];
+    const uint32_t s = dgoff[g], e = dgoff[g + 1];
     if (e > s) {
-      i0 = s >> 5;
-      i1 = (e + 31u) >> 5;
+      L.i0 = s >> 5;
+      L.nw = ((e + 31u) >> 5) - L.i0;
+      L.mf = range_mask(L.i0, s, e, prof);
+      L.ml = range_mask(L.i0 + L.nw - 1u, s, e, prof);
     }
   }
-  const uint64_t j0 = static_cast<uint64_t>(blockIdx.y) * kNeRowsPerBlock;
-  const uint64_t j1 = j0 + kNeRowsPerBlock < Qn ? j0 + kNeRowsPerBlock : Qn;
-  // The range masks of this graph's words are the same for every row: a graph
-  // of <= 65 vertices spans at most kNeWords words, whose masks are computed
-  // once (a zero mask, REF_PTX's dropped last word, is not even loaded).
-  constexpr uint32_t kNeWords = 3;
-  const bool few = i1 - i0 <= kNeWords;
-  uint32_t mk[kNeWords];
-#pragma unroll
-  for (uint32_t w = 0; w < kNeWords; ++w) mk[w] = few && i0 + w < i1 ? range_mask(i0 + w, s, e, prof) : 0u;
-  for (uint64_t j = j0; j < j1; j += kNeBatch) {
-    uint32_t acc[kNeBatch];
-#pragma unroll
-    for (uint32_t k = 0; k < kNeBatch; ++k) acc[k] = 0;
-    if (few) {
-#pragma unroll
-      for (uint32_t w = 0; w < kNeWords; ++w) {
-        if (!mk[w]) continue;
-        const uint32_t* col = bits + j * Wp + i0 + w;
-#pragma unroll
-        for (uint32_t k = 0; k < kNeBatch; ++k)
-          if (j + k < j1) acc[k] |= col[k * Wp] & mk[w];
+  L.m0 = L.nw ? L.mf : 0u;
+  L.m1 = L.nw == 2u ? L.ml : (L.nw == 3u ? 0xFFFFFFFFu : 0u);
+  L.m2 = L.nw == 3u ? L.ml : 0u;
+  L.o1 = L.nw > 1u ? 1u : 0u;
+  L.o2 = L.nw > 2u ? 2u : L.o1;
+  const bool wide = !__all_sync(0xFFFFFFFFu, L.nw <= 3u);
+  // the CTA's word span, 16-byte aligned at both ends (Wp is a multiple of 32)
+  const uint32_t g_hi = g_lo + kNeThreads < G ? g_lo + kNeThreads : G;
+  const uint32_t ws = (dgoff[g_lo] >> 5) & ~3u;
+  uint32_t we = (((dgoff[g_hi] + 31u) >> 5) + 3u) & ~3u;
+  if (we > Wp) we = static_cast<uint32_t>(Wp);
+  const uint32_t SW = we > ws ? we - ws : 0u;
+  const uint32_t rs_fit = SW ? kNeStageWords / SW : 0u;
+  const uint32_t RS = rs_fit < 32u ? rs_fit : 32u;  // rows per stage (one copy per lane of warp 0)
+  const bool staged = RS > 0u;
+  const uint32_t a = L.nw ? L.i0 - ws : 0u;  // the lane's first word within a staged row
+  const uint64_t j0 = static_cast<uint64_t>(blockIdx.y) * kNeRowsPerCta;
+  const uint64_t j1 = j0 + kNeRowsPerCta < Qn ? j0 + kNeRowsPerCta : Qn;
+  const uint32_t nrows = static_cast<uint32_t>(j1 - j0);
+  const uint32_t nch = staged ? (nrows + RS - 1u) / RS : 1u;
+  const uint32_t chunk_rows = staged ? RS : nrows;
+
+  // warp 0 (lane 0's copy is the one used): stages whose phase lane 0 did not
+  // see complete, and the parity of that phase
+  uint32_t failed = 0, failed_par = 0;
+  if (staged) {
+    if (threadIdx.x == 0)
+      for (uint32_t st = 0; st < kNeStages; ++st) {
+        mbar_init(&s_bar[st], 1);
+        s_live[st] = 0u;
+      }
+    __syncthreads();
+    if (warp == 0)
+      for (uint32_t c = 0; c < nch && c < kNeStages; ++c) ne_issue(c, lane, RS, SW, nrows, j0, ws, Wp, bits, s_stage, s_bar, s_live);
+    __syncthreads();
+  }
+  uint32_t* ne_out = NE + j0 * GW + gw;
+  for (uint32_t c = 0; c < nch; ++c) {
+    const uint32_t st = c % kNeStages;
+    const uint32_t r0 = c * chunk_rows;
+    const uint32_t nr = nrows - r0 < chunk_rows ? nrows - r0 : chunk_rows;
+    const bool live = staged && s_live[st];
+    const bool have = live && mbar_wait_sleep(&s_bar[st], (c / kNeStages) & 1u, kNeSleepNs, kNePolls);
+    const uint32_t* srow = s_stage + st * kNeStageWords + a;
+    const uint32_t* grow = bits + (j0 + r0) * Wp + L.i0;
+    // lane r keeps the NE word of the chunk's row r; the chunk's words are
+    // stored together (one row per lane)
+    uint32_t mine = 0;
+    if (__all_sync(0xFFFFFFFFu, have) && !wide) {
+      // words 1 and 2 are read even where the graph has fewer (masked to
+      // zero; the ring has kNePadWords of slack past its end)
+      const uint32_t* p = srow;
+#pragma unroll 4
+      for (uint32_t r = 0; r < nr; ++r, p += SW) {
+        const uint32_t acc = (p[0] & L.m0) | (p[1] & L.m1) | (p[2] & L.m2);
+        const uint32_t word = __ballot_sync(0xFFFFFFFFu, acc != 0u);
+        mine = lane == r ? word : mine;
       }
     } else {
-      for (uint32_t i = i0; i < i1; ++i) {
-        const uint32_t m = range_mask(i, s, e, prof);
-        const uint32_t* col = bits + j * Wp + i;
-#pragma unroll
-        for (uint32_t k = 0; k < kNeBatch; ++k)
-          if (j + k < j1) acc[k] |= col[k * Wp] & m;
+      for (uint32_t r = 0; r < nr; ++r) {
+        const uint32_t* row = have ? srow + r * SW : grow + static_cast<uint64_t>(r) * Wp;
+        const bool any = L.nw && (wide ? ne_any_wide(row, L) : ne_any_few(row, L));
+        const uint32_t word = __ballot_sync(0xFFFFFFFFu, any);
+        if (r < 32u) mine = lane == r ? word : mine;
+        else if (lane == 0 && gw < GW) ne_out[static_cast<uint64_t>(r0 + r) * GW] = word;  // unstaged chunks only
       }
     }
-#pragma unroll
-    for (uint32_t k = 0; k < kNeBatch; ++k) {
-      const uint32_t word = __ballot_sync(0xFFFFFFFFu, acc[k] != 0);
-      if (lane == 0 && j + k < j1) NE[(j + k) * GW + gw] = word;
+    if (lane < nr && gw < GW) ne_out[static_cast<uint64_t>(r0 + lane) * GW] = mine;
+    if (staged) {
+      // once every warp is done with this stage, warp 0 refills it with chunk
+      // c + kNeStages, unless lane 0 did not see a copy complete (then no
+      // stage is refilled again and readers of the unfilled chunks, finding
+      // s_live clear, read global memory)
+      __syncthreads();
+      if (warp == 0) {
+        if (lane == 0 && live && !have) {
+          failed |= 1u << st;
+          failed_par |= ((c / kNeStages) & 1u) << st;
+        }
+        const bool stop = __shfl_sync(0xFFFFFFFFu, failed, 0) != 0u;
+        if (c + kNeStages < nch && !stop) ne_issue(c + kNeStages, lane, RS, SW, nrows, j0, ws, Wp, bits, s_stage, s_bar, s_live);
+        else if (lane == 0) s_live[st] = 0u;
+      }
     }
   }
+  // a copy whose wait ran out may still be in flight: wait for it again
+  // (bounded) before the CTA's shared memory is released
+  if (threadIdx.x == 0 && failed)
+    for (uint32_t st = 0; st < kNeStages; ++st)
+      if (failed >> st & 1u) mbar_wait_sleep(&s_bar[st], failed_par >> st & 1u, kNeSleepNs, kNePolls);
 }
 
 // Warp per 32 data graphs; lanes take query graphs 32 at a time.
@@ -161,6 +271,17 @@ __global__ void k_gmcr_fill(const uint32_t* __restrict__ admit, uint32_t GW, uin
 }
 
 }  // namespace
+
+// The non-empty pass over the bitset into NE [Qn][GW].
+static int launch_gmcr_ne(Queue* q, const Candidates* c, const Graph* data, uint64_t Qn, uint32_t* NE) {
+  const uint32_t G = data->num_graphs;
+  const uint32_t GW = (G + 31u) / 32u;
+  const dim3 grid((G + kNeThreads - 1u) / kNeThreads, static_cast<unsigned>((Qn + kNeRowsPerCta - 1) / kNeRowsPerCta));
+  if (grid.y > 65535u) return fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", static_cast<unsigned long long>(Qn));
+  SIGMO_TRY(allow_max_dynamic_smem(reinterpret_cast<const void*>(k_gmcr_ne), q->device));
+  k_gmcr_ne<<<grid, kNeThreads, kNeSmemBytes, q->stream>>>(c->bits, c->Wp, Qn, data->graph_offsets, G, GW, q->opts.profile, NE);
+  return check_launch(q, "k_gmcr_ne");
+}
 
 // Admission, counts, scan and fill from an NE matrix (rows per query vertex,
 // or per class when cls != nullptr).  With sync_total the total is read back
@@ -255,12 +376,7 @@ int launch_gmcr(Queue* q, const Graph* query, const Graph* data, const Candidate
   uint32_t* NE = static_cast<uint32_t*>(ne);
   int rc = SIGMO_OK;
   if (G && query->num_graphs && Qn) {
-    dim3 grid_ne((GW + 7u) / 8u, static_cast<unsigned>((Qn + kNeRowsPerBlock - 1) / kNeRowsPerBlock));
-    if (grid_ne.y > 65535u) rc = fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", (unsigned long long)Qn);
-    if (!rc) {
-      k_gmcr_ne<<<grid_ne, 256, 0, q->stream>>>(c->bits, c->Wp, Qn, data->graph_offsets, G, GW, q->opts.profile, NE);
-      rc = check_launch(q, "k_gmcr_ne");
-    }
+    rc = launch_gmcr_ne(q, c, data, Qn, NE);
   }
   if (!rc) rc = launch_gmcr_from_ne(q, query, data, NE, nullptr, m, sync_total, capacity_hint);
   dev_free(q, ne);
@@ -341,10 +457,7 @@ extern "C" int sigmo_gmcr_generate_noalloc(sigmo_queue_t q, sigmo_graph_t query,
   // d_offsets[0] must start at zero; NE, admit and counts are fully written below.
   SIGMO_CUDA_TRY(cudaMemsetAsync(d_offsets, 0, sizeof(uint32_t) * (G + 1ull), q->stream));
   if (G && QG && Qn) {
-    dim3 grid_ne((GW + 7u) / 8u, static_cast<unsigned>((Qn + kNeRowsPerBlock - 1) / kNeRowsPerBlock));
-    if (grid_ne.y > 65535u) return fail(SIGMO_ERR_DOMAIN, "too many query vertices (%llu)", static_cast<unsigned long long>(Qn));
-    k_gmcr_ne<<<grid_ne, 256, 0, q->stream>>>(c->bits, c->Wp, Qn, data->graph_offsets, G, GW, q->opts.profile, NE);
-    SIGMO_TRY(check_launch(q, "k_gmcr_ne"));
+    SIGMO_TRY(launch_gmcr_ne(q, c, data, Qn, NE));
     k_gmcr_admit<<<grid_for(GW * 32ull, 256, 148u * 16u), 256, 0, q->stream>>>(NE, GW, query->graph_offsets, QG, G, nullptr,
                                                                                 admit, counts);
     SIGMO_TRY(check_launch(q, "k_gmcr_admit"));

@@ -7,6 +7,7 @@
 // a BFS level is an OR of rows selected by the frontier's bits.
 #include <cuda_runtime.h>
 
+#include "bulk.cuh"
 #include "internal.hpp"
 
 namespace sigmo_b200 {
@@ -206,41 +207,6 @@ __global__ void k_sig_refine_exact(uint64_t N, const uint32_t* __restrict__ goff
 // wait is bounded; past the bound the range is computed from global memory
 // (results are the same either way) and the CTA stops staging.
 constexpr uint32_t kSigRange = 256;
-constexpr uint32_t kSigSpinLimit = 1u << 22;
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a), "r"(bytes) : "memory");
-}
-// Bulk global -> shared copy of `bytes` (multiple of 16; both addresses
-// 16-byte aligned), its completion counted on `bar`.
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d), "l"(src),
-               "r"(bytes), "r"(b)
-               : "memory");
-}
-// Waits (bounded) for phase `parity` of `bar` to complete; false if it did not.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
-  for (uint32_t i = 0; i < kSigSpinLimit; ++i) {
-    uint32_t done = 0;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
 template <int AW, bool EXACT>
 __global__ void __launch_bounds__(kSigRange) k_sig_all_staged(uint64_t N, const uint32_t* __restrict__ goff,
                                                               const uint32_t* __restrict__ node_graph,
