@@ -70,3 +70,29 @@ def test_batched_form_refuses_ref_x86():
     with pytest.raises(sb.SigmoError) as ei:
         sb.match_batched(queue, qg, dg, 3, False, None, sb.GMCR(queue))
     assert ei.value.code == 4
+
+
+def test_ptx_shift_instructions_clamp(tmp_path):
+    """REF_PTX rests on one hardware fact: the PTX shift instructions that the
+    reference's over-wide shifts become on an NVIDIA GPU (shr.u32 / shl.b32 in
+    the range masks, candidates.hpp:91-99; shl.b64 in the Bitset,
+    utils.hpp:71-73) give 0 for a run-time count >= the register width, where
+    x86-64 takes the count modulo the width.  This runs those instructions on
+    the device (tests/ptx_shift_probe.cu, built here with nvcc)."""
+    import shutil
+    import subprocess
+
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    exe = tmp_path / "ptx_shift_probe"
+    src = Path(__file__).resolve().parent / "ptx_shift_probe.cu"
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    rows = [tuple(int(x) for x in line.split()) for line in out if line.strip()]
+    assert len(rows) == 12
+    m32 = 0xFFFFFFFF
+    for n, shr, shl, shl64 in rows:
+        assert shr == (m32 >> n if n < 32 else 0), n
+        assert shl == ((m32 << n) & m32 if n < 32 else 0), n
+        assert shl64 == (1 << n if n < 64 else 0), n
+    # the x86-64 reading differs exactly where the counts are over-wide
+    assert any(n >= 32 and shr != m32 >> (n & 31) for n, shr, _, _ in rows)
