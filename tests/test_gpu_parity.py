@@ -452,3 +452,49 @@ def test_query_batch_admitted_in_groups():
     ref = _oracle(q, d, 4, oracle.REF_PTX, False)
     got = run_both_batched(q, d, 4, oracle.REF_PTX, False)
     _check(got, ref, "grouped admission")
+
+
+@pytest.mark.parametrize("prof", (oracle.REF_PTX, oracle.REF_X86))
+def test_gmcr_pass_span_shapes(prof):
+    """The plain form's GMCR pass stages each CTA's word span of 256 data
+    graphs in shared memory: molecules of 600-900 atoms (spans at and over one
+    stage, so some CTAs read global memory, and graphs spanning up to 29
+    words; 200-256 atoms under REF_X86, a few rows per stage), and molecules
+    of 1-3 atoms (up to 32 graphs per bitset word).
+    Bitset and GMCR against the oracle; the small molecules also through the
+    join."""
+    q = sb.generate_queries(20, 3, 8, seed=53)
+    # REF_X86's stage calls take graphs of up to 256 vertices
+    big = (sb.generate_molecules(300, 600, 900, seed=51, median=750.0) if prof == oracle.REF_PTX
+           else sb.generate_molecules(600, 200, 256, seed=51, median=228.0))
+    for name, d in (("big", big), ("tiny", sb.generate_molecules(6000, 1, 3, seed=52, median=2.0))):
+        sd, sq = oracle.generate_signatures(d), oracle.generate_signatures(q)
+        bits = oracle.filter_candidates(q, d)
+        rd, rq = oracle.new_reach(len(sd), prof), oracle.new_reach(len(sq), prof)
+        for r in (1, 2):
+            sd = oracle.refine_signatures(d, r, prof, sd, rd)
+            sq = oracle.refine_signatures(q, r, prof, sq, rq)
+            bits = oracle.refine_candidates(q, d, sq, sd, bits)
+        off, idx = oracle.gmcr(q, d, bits, prof)
+        assert len(idx) > 0, name
+        queue = sb.Queue(0, profile=prof)
+        qg, dg = sb.createDeviceCSRGraph(queue, q), sb.createDeviceCSRGraph(queue, d)
+        cand = sb.Candidates(queue, qg.total_nodes, dg.total_nodes)
+        sig = sb.Signature(queue, dg.total_nodes, qg.total_nodes)
+        sig.generateDataSignatures(dg)
+        sig.generateQuerySignatures(qg)
+        sb.filterCandidates(queue, qg, dg, sig, cand)
+        for r in (1, 2):
+            sig.refineDataSignatures(dg, r)
+            sig.refineQuerySignatures(qg, r)
+            sb.refineCandidates(queue, qg, dg, sig, cand)
+        assert np.array_equal(cand.getHostCandidates(), bits), name
+        gm = sb.GMCR(queue)
+        gm.generateGMCR(qg, dg, cand)
+        goff, gidx = gm.getGMCR()
+        assert np.array_equal(goff, off) and np.array_equal(gidx, idx), name
+        if name == "tiny":
+            nm = np.zeros(1, np.uint64)
+            _, per = sb.joinCandidates(queue, qg, dg, cand, gm, nm, True, per_pair=True)
+            ref_total, ref_per = oracle.join(q, d, bits, off, idx, prof, True)
+            assert int(nm[0]) == ref_total and np.array_equal(per, ref_per), name
