@@ -231,40 +231,38 @@ __global__ void k_gmcr_admit(const uint32_t* __restrict__ NE, uint32_t GW, const
   }
 }
 
-// Segment fill: lane = data graph; query ids visited in ascending order, so
-// every segment is sorted.
+// Segment fill.  A warp owns 32 consecutive data graphs (one admission word
+// column) and walks the query graphs 32 at a time: lane l loads the word of
+// query q0 + l, then for each of the 32 graphs a vote gives the chunk's
+// admitted queries in ascending order, which the lanes write to consecutive
+// entries of that graph's segment (coalesced); lane j keeps graph j's write
+// position.  Every segment is sorted.
 __global__ void k_gmcr_fill(const uint32_t* __restrict__ admit, uint32_t GW, uint32_t QG, uint32_t G,
                             const uint32_t* __restrict__ offsets, uint32_t* __restrict__ indices,
                             uint32_t* __restrict__ pair_graph, uint64_t capacity) {
   const unsigned lane = threadIdx.x & 31u;
+  const uint32_t lt = (1u << lane) - 1u;
   const uint32_t warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t gw = warp; gw < GW; gw += nwarps) {
-    const uint32_t g = gw * 32u + lane;
-    uint64_t cur = g < G ? offsets[g] : 0;
-    uint32_t q = 0;
-    for (; q + 8 <= QG; q += 8) {  // eight admission words in flight
-      uint32_t a[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) a[k] = admit[static_cast<uint64_t>(q + k) * GW + gw];
-#pragma unroll
-      for (int k = 0; k < 8; ++k)
-        if ((a[k] >> lane) & 1u) {
-          if (cur < capacity) {
-            indices[cur] = q + k;
-            if (pair_graph) pair_graph[cur] = g;
+    const uint32_t g_own = gw * 32u + lane;
+    uint64_t cur = g_own < G ? offsets[g_own] : 0;  // lane j: next entry of graph gw * 32 + j
+    const uint32_t in_tile = G - gw * 32u < 32u ? G - gw * 32u : 32u;
+    for (uint32_t q0 = 0; q0 < QG; q0 += 32) {
+      const uint32_t q = q0 + lane;
+      const uint32_t w = q < QG ? admit[static_cast<uint64_t>(q) * GW + gw] : 0u;
+      for (uint32_t j = 0; j < in_tile; ++j) {
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, (w >> j) & 1u);
+        if (!m) continue;
+        const uint64_t base = __shfl_sync(0xFFFFFFFFu, cur, j);
+        if ((m >> lane) & 1u) {
+          const uint64_t pos = base + __popc(m & lt);
+          if (pos < capacity) {
+            indices[pos] = q;
+            if (pair_graph) pair_graph[pos] = gw * 32u + j;
           }
-          ++cur;
         }
-    }
-    for (; q < QG; ++q) {
-      const uint32_t a = admit[static_cast<uint64_t>(q) * GW + gw];
-      if ((a >> lane) & 1u) {
-        if (cur < capacity) {
-          indices[cur] = q;
-          if (pair_graph) pair_graph[cur] = g;
-        }
-        ++cur;
+        if (lane == j) cur += __popc(m);
       }
     }
   }
