@@ -395,6 +395,14 @@ def run_serving(args, d, wl, local):
         adm = [b["gathered_plane_bytes"] / (b["ms_filter"] / 1e3) / 1e9 for b in by_batch.values()
                if b["gathered_plane_bytes"] and b["ms_filter"] > 0]
         p99 = float(np.percentile(lat, 99))
+
+        def stage_medians(batches):
+            if not batches:
+                return None
+            return {k: round(float(np.median([b[f] for b in batches])), 3)
+                    for k, f in (("device", "ms_device"), ("filter", "ms_filter"), ("mapping", "ms_mapping"),
+                                 ("join", "ms_join"), ("queries", "batch_queries"))} | {"batches": len(batches)}
+
         return {
             "requests": n_req, "arrival_rate_per_s": rate, "queries_per_request": "uniform 1-64",
             "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p95": round(float(np.percentile(lat, 95)), 3),
@@ -407,6 +415,9 @@ def run_serving(args, d, wl, local):
             "batches": st1["batches"] - st0["batches"],
             "mean_requests_per_batch": round((st1["requests_completed"] - st0["requests_completed"]) /
                                              max(1, st1["batches"] - st0["batches"]), 2),
+            "batch_stages_ms_median": {"all": stage_medians(list(by_batch.values())),
+                                       "batches_of_48_plus_queries": stage_medians(
+                                           [b for b in by_batch.values() if b["batch_queries"] >= 48])},
             "admission_gather_gbs_median": round(float(np.median(adm)), 1) if adm else None,
             "admission_gather_frac_of_hbm": round(float(np.median(adm)) / hbm, 4) if adm else None,
             "clocks": clk.summary(),
