@@ -242,15 +242,14 @@ int plan_groups(Queue* q, Graph* query, uint32_t AW, const std::vector<uint32_t>
   PlaneProgram& pp = query->pp;
   const uint32_t QG = query->num_graphs, K = pp.K, C = pp.C, R = pp.R;
   std::vector<uint32_t> plane_mark(K, 0), class_mark(C, 0);  // stamp = group number + 1
-  uint32_t stamp = 0, Kg = 0, Cg = 0, q0 = 0;
+  uint32_t stamp = 0, Kg = 0, q0 = 0;
   std::vector<std::pair<uint32_t, uint32_t>> ranges;
-  auto query_adds = [&](uint32_t qg, uint32_t* dk, uint32_t* dc) {
-    *dk = *dc = 0;
+  auto query_adds = [&](uint32_t qg, uint32_t* dk) {  // planes query qg adds to the group
+    *dk = 0;
     std::vector<uint32_t> seen_planes;
     for (uint32_t e = off[qg]; e < off[qg + 1]; ++e) {
       const uint32_t c = list[e];
       if (class_mark[c] == stamp) continue;
-      ++*dc;
       for (uint32_t i = pp.h_prog_off[c]; i < pp.h_prog_off[c + 1]; ++i) {
         const uint32_t k = pp.h_prog[i];
         if (plane_mark[k] != stamp && std::find(seen_planes.begin(), seen_planes.end(), k) == seen_planes.end()) {
@@ -265,7 +264,6 @@ int plan_groups(Queue* q, Graph* query, uint32_t AW, const std::vector<uint32_t>
       const uint32_t c = list[e];
       if (class_mark[c] == stamp) continue;
       class_mark[c] = stamp;
-      ++Cg;
       for (uint32_t i = pp.h_prog_off[c]; i < pp.h_prog_off[c + 1]; ++i)
         if (plane_mark[pp.h_prog[i]] != stamp) {
           plane_mark[pp.h_prog[i]] = stamp;
@@ -275,16 +273,16 @@ int plan_groups(Queue* q, Graph* query, uint32_t AW, const std::vector<uint32_t>
   };
   stamp = 1;
   for (uint32_t qg = 0; qg < QG; ++qg) {
-    uint32_t dk, dc;
-    query_adds(qg, &dk, &dc);
-    if (qg > q0 && planes_admit_smem(Kg + dk, AW, Cg + dc) > kGroupSmemBudget) {
+    uint32_t dk;
+    query_adds(qg, &dk);
+    if (qg > q0 && planes_admit_smem(Kg + dk, AW) > kGroupSmemBudget) {
       ranges.emplace_back(q0, qg);
       ++stamp;
-      Kg = Cg = 0;
+      Kg = 0;
       q0 = qg;
     }
     take(qg);
-    if (planes_admit_smem(Kg, AW, Cg) > 200u * 1024u)
+    if (planes_admit_smem(Kg, AW) > 200u * 1024u)
       return fail(SIGMO_ERR_DOMAIN, "query graph %u alone needs more than one admission tile of shared memory", qg);
   }
   ranges.emplace_back(q0, QG);
@@ -340,7 +338,7 @@ int plan_groups(Queue* q, Graph* query, uint32_t AW, const std::vector<uint32_t>
       if (k >= grp.K) return fail(SIGMO_ERR_INVALID, "internal: group %zu plane %u outside its %u planes", gi, k, grp.K);
     for (uint32_t c : qc)
       if (c >= grp.C) return fail(SIGMO_ERR_INVALID, "internal: group %zu class %u outside its %u classes", gi, c, grp.C);
-    if (planes_admit_smem(grp.K, AW, grp.C) > 200u * 1024u)
+    if (planes_admit_smem(grp.K, AW) > 200u * 1024u)
       return fail(SIGMO_ERR_DOMAIN, "group %zu needs more than one admission tile of shared memory", gi);
     grp.nlab = nlab;
     grp.n_qc = qc.size();
@@ -399,7 +397,7 @@ int order_classes(Queue* q, Graph* query, Graph* data) {
   pp.h_qc_n = list.size();
   free_groups(q, &pp);
   const uint32_t AW = data->adj_words;
-  if (planes_admit_smem(pp.K, AW, pp.C) > kGroupSmemBudget) SIGMO_TRY(plan_groups(q, query, AW, off, list));
+  if (planes_admit_smem(pp.K, AW) > kGroupSmemBudget) SIGMO_TRY(plan_groups(q, query, AW, off, list));
   SIGMO_CUDA_TRY(cudaStreamSynchronize(q->stream));  // host vectors go out of scope
   pp.qc_for = data;
   pp.qc_stamp = data->stamp;
@@ -729,7 +727,7 @@ int match_batched(Queue* q, Graph* query, Graph* data, uint32_t R, int find_firs
   if (prc == SIGMO_ERR_DOMAIN) prc = SIGMO_OK;  // a query graph too large for a tile: bitset route
   else if (prc) return prc;
   const bool planes_fit = query->pp.qc_for == data && (!query->pp.groups.empty() ||
-                                                       planes_admit_smem(query->pp.K, data->adj_words, query->pp.C) <= 200u * 1024u);
+                                                       planes_admit_smem(query->pp.K, data->adj_words) <= 200u * 1024u);
   const bool bitset_route = materialize || !planes_fit;
   if (!rc && bitset_route && data->vertex_base)
     rc = fail(SIGMO_ERR_DOMAIN, "a shard (vertex base %u) runs on the planes route only; this batch needs the bitset route",

@@ -264,13 +264,13 @@ int launch_planes_admit(Queue* q, const Graph* query, const Graph* data, const u
 // its per-graph admitted counts are added to counts.
 int launch_planes_admit_group(Queue* q, const Graph* query, const Graph* data, const uint64_t* sig_all, uint32_t R,
                               const PlaneGroup& grp, uint32_t K_total, uint64_t* planes, uint32_t* admit, uint32_t* counts);
-// Shared memory of one k_planes_admit tile for K planes and C classes.
+// Shared memory of one k_planes_admit tile budgeted for a query group's planes.
 constexpr size_t kGroupSmemBudget = 96u * 1024u;
 // The same admission with the tile's planes gathered from resident planes
 // (row_map[k] = resident row of the batch's plane k).
 int launch_planes_admit_resident(Queue* q, const Graph* query, const Graph* data, const ResidentPlanes& rp,
                                  const PlaneProgram& pp, const uint32_t* row_map, uint32_t* admit, uint32_t* counts);
-size_t planes_admit_smem(uint32_t K, uint32_t AW, uint32_t C);
+size_t planes_admit_smem(uint32_t K, uint32_t AW);
 // GMCR from admission words admit[query graph][data graph / 32] and the
 // admitted count of every data graph (scan, total, sorted fill).
 int launch_gmcr_from_admit(Queue* q, const Graph* query, const Graph* data, const uint32_t* admit, const uint32_t* counts,

@@ -103,9 +103,10 @@ __device__ __forceinline__ void build_graph_planes(uint64_t* tile, uint32_t gl, 
 // Warps take query graphs; a query's classes are visited in the order the
 // host chose (rarest label first, longer programs first), so most queries
 // are rejected for all 32 graphs after one or two classes and stop there.
-// NE(c) is computed at most once per tile per warp race (a shared-memory
-// cache with a valid bit per class), and a class's AND chain stops as soon as
-// it is zero in all 32 graphs.  The per-graph admitted counts (the GMCR
+// A class's AND chain stops as soon as it is zero in all 32 graphs.  NE(c)
+// is evaluated for each query that reaches it: classes are rarely shared
+// between queries, and without a per-class cache in shared memory four CTAs
+// fit on an SM instead of three.  The per-graph admitted counts (the GMCR
 // segment lengths) are summed in shared memory.  Queries of one vertex are
 // never admitted (the reference's mapping skips them, gmcr.hpp:100).
 constexpr uint32_t kAdmitWarps = 16;
@@ -163,20 +164,16 @@ __device__ __forceinline__ void gather_tile_async(uint64_t* dst, const uint64_t*
 }
 
 // Shared-memory layout of k_planes_admit (in u64 units for the tiles):
-//   tile buffer(s) [1 or 2][K * AW * 32] u64, ne_word[C], ne_valid[CW],
-//   s_map[K] (gather), then the staged class lists when they fit:
+//   tile buffer(s) [1 or 2][K * AW * 32] u64, s_map[K] (gather), then the
+//   staged class lists when they fit:
 //   qc_off[QG + 1], qc[n_qc], prog_off[C + 1] (u32), prog[n_prog] (u16).
 struct AdmitSmem {
-  size_t tiles, ne_word, ne_valid, map, lists, total;
+  size_t tiles, map, lists, total;
 };
-__host__ __device__ inline AdmitSmem admit_smem_layout(uint32_t K, uint32_t AW, uint32_t C, bool gather, size_t list_bytes) {
+__host__ __device__ inline AdmitSmem admit_smem_layout(uint32_t K, uint32_t AW, bool gather, size_t list_bytes) {
   AdmitSmem l{};
   l.tiles = 0;
   size_t off = static_cast<size_t>(gather ? 2 : 1) * K * AW * 32 * 8;
-  l.ne_word = off;
-  off += 4ull * C;
-  l.ne_valid = off;
-  off += 4ull * ((C + 31) / 32);
   l.map = off;
   off += gather ? 4ull * K : 0;
   off = (off + 15) & ~static_cast<size_t>(15);
@@ -201,12 +198,10 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
   constexpr uint32_t kRow = AW * 32u;
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t GW = (G + 31u) / 32u;
-  const uint32_t words = K * AW, CW = (C + 31u) / 32u;
+  const uint32_t words = K * AW;
   const size_t list_bytes = stage_lists ? 4ull * (QG + 1 + n_qc + C + 1) + 2ull * n_prog : 0;
-  const AdmitSmem L = admit_smem_layout(K, AW, C, GATHER, list_bytes);
+  const AdmitSmem L = admit_smem_layout(K, AW, GATHER, list_bytes);
   uint64_t* tiles = reinterpret_cast<uint64_t*>(smem_raw);
-  uint32_t* ne_word = reinterpret_cast<uint32_t*>(smem_raw + L.ne_word);
-  uint32_t* ne_valid = reinterpret_cast<uint32_t*>(smem_raw + L.ne_valid);
   uint32_t* s_map = reinterpret_cast<uint32_t*>(smem_raw + L.map);
   // per-batch constants: the row map and (when they fit) the class lists
   const uint32_t* qc_off = g_qc_off;
@@ -241,7 +236,6 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
       __syncthreads();  // the previous tile is no longer read
       fill_tile<AW, false>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, base, nullptr, 0, nullptr);
     }
-    for (uint32_t i = threadIdx.x; i < CW; i += blockDim.x) ne_valid[i] = 0;
     if (threadIdx.x < 32) tile_cnt[threadIdx.x] = 0;
     __syncthreads();
     if (!GATHER) {
@@ -268,48 +262,37 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
       const uint32_t e1 = qc_off[qg + 1];
       for (uint32_t e = qc_off[qg]; e < e1 && alive; ++e) {
         const uint32_t c = qc[e];
-        uint32_t word;
-        if ((*reinterpret_cast<volatile uint32_t*>(&ne_valid[c >> 5]) >> (c & 31u)) & 1u) {
-          __threadfence_block();
-          word = *reinterpret_cast<volatile uint32_t*>(&ne_word[c]);
-        } else {
-          uint64_t m[AW];
+        uint64_t m[AW];
 #pragma unroll
-          for (int w = 0; w < AW; ++w) m[w] = ~0ull;
-          bool any = true;
-          const uint32_t k1 = prog_off[c + 1];
-          // two planes per step between the warp votes
-          uint32_t k = prog_off[c];
-          bool live = true;
-          for (; k + 2 <= k1; k += 2) {
-            const uint32_t off0 = static_cast<uint32_t>(prog[k]) * kRow, off1 = static_cast<uint32_t>(prog[k + 1]) * kRow;
-            any = false;
+        for (int w = 0; w < AW; ++w) m[w] = ~0ull;
+        bool any = true;
+        const uint32_t k1 = prog_off[c + 1];
+        // two planes per step between the warp votes
+        uint32_t k = prog_off[c];
+        bool live = true;
+        for (; k + 2 <= k1; k += 2) {
+          const uint32_t off0 = static_cast<uint32_t>(prog[k]) * kRow, off1 = static_cast<uint32_t>(prog[k + 1]) * kRow;
+          any = false;
 #pragma unroll
-            for (int w = 0; w < AW; ++w) {
-              m[w] &= tl[off0 + 32 * w] & tl[off1 + 32 * w];
-              any |= m[w] != 0;
-            }
-            if (!__any_sync(0xFFFFFFFFu, any)) {
-              live = false;
-              break;
-            }
+          for (int w = 0; w < AW; ++w) {
+            m[w] &= tl[off0 + 32 * w] & tl[off1 + 32 * w];
+            any |= m[w] != 0;
           }
-          if (live && k < k1) {
-            const uint32_t off = static_cast<uint32_t>(prog[k]) * kRow;
-            any = false;
-#pragma unroll
-            for (int w = 0; w < AW; ++w) {
-              m[w] &= tl[off + 32 * w];
-              any |= m[w] != 0;
-            }
-          }
-          word = __ballot_sync(0xFFFFFFFFu, any);
-          if (lane == 0) {
-            *reinterpret_cast<volatile uint32_t*>(&ne_word[c]) = word;
-            __threadfence_block();
-            atomicOr(&ne_valid[c >> 5], 1u << (c & 31u));
+          if (!__any_sync(0xFFFFFFFFu, any)) {
+            live = false;
+            break;
           }
         }
+        if (live && k < k1) {
+          const uint32_t off = static_cast<uint32_t>(prog[k]) * kRow;
+          any = false;
+#pragma unroll
+          for (int w = 0; w < AW; ++w) {
+            m[w] &= tl[off + 32 * w];
+            any |= m[w] != 0;
+          }
+        }
+        const uint32_t word = __ballot_sync(0xFFFFFFFFu, any);
         alive &= word;
       }
       if (lane == 0) admit[static_cast<uint64_t>(qg) * GW + gw] = alive;
@@ -401,8 +384,8 @@ int ensure_label_hist(Queue* q, Graph* g) {
   return rc;
 }
 
-size_t planes_admit_smem(uint32_t K, uint32_t AW, uint32_t C) {
-  return admit_smem_layout(K, AW, C, false, 0).total;
+size_t planes_admit_smem(uint32_t K, uint32_t AW) {
+  return admit_smem_layout(K, AW, false, 0).total;
 }
 
 namespace {
@@ -424,10 +407,10 @@ int admit_launch(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t 
   const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, QG = v.QG;
   const uint32_t n_qc = static_cast<uint32_t>(v.n_qc), n_prog = static_cast<uint32_t>(v.n_prog);
   const size_t list_bytes = 4ull * (QG + 1 + n_qc + v.C + 1) + 2ull * n_prog;
-  const size_t base = admit_smem_layout(v.K, AW, v.C, GATHER, 0).total;
+  const size_t base = admit_smem_layout(v.K, AW, GATHER, 0).total;
   // stage the class lists when the block still fits three to an SM
   const int stage = base + list_bytes <= 72u * 1024u ? 1 : 0;
-  const size_t smem = admit_smem_layout(v.K, AW, v.C, GATHER, stage ? list_bytes : 0).total;
+  const size_t smem = admit_smem_layout(v.K, AW, GATHER, stage ? list_bytes : 0).total;
   if (smem > 220u * 1024u) return fail(SIGMO_ERR_DOMAIN, "k_planes_admit needs %zu bytes of shared memory", smem);
   const unsigned block = 32u * kAdmitWarps;
   int per_sm = 0, sms = 0;
