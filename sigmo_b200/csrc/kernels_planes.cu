@@ -267,15 +267,16 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
         for (int w = 0; w < AW; ++w) m[w] = ~0ull;
         bool any = true;
         const uint32_t k1 = prog_off[c + 1];
-        // two planes per step between the warp votes
+        // four planes per step between the warp votes
         uint32_t k = prog_off[c];
         bool live = true;
-        for (; k + 2 <= k1; k += 2) {
+        for (; k + 4 <= k1; k += 4) {
           const uint32_t off0 = static_cast<uint32_t>(prog[k]) * kRow, off1 = static_cast<uint32_t>(prog[k + 1]) * kRow;
+          const uint32_t off2 = static_cast<uint32_t>(prog[k + 2]) * kRow, off3 = static_cast<uint32_t>(prog[k + 3]) * kRow;
           any = false;
 #pragma unroll
           for (int w = 0; w < AW; ++w) {
-            m[w] &= tl[off0 + 32 * w] & tl[off1 + 32 * w];
+            m[w] &= (tl[off0 + 32 * w] & tl[off1 + 32 * w]) & (tl[off2 + 32 * w] & tl[off3 + 32 * w]);
             any |= m[w] != 0;
           }
           if (!__any_sync(0xFFFFFFFFu, any)) {
@@ -284,13 +285,14 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
           }
         }
         if (live && k < k1) {
-          const uint32_t off = static_cast<uint32_t>(prog[k]) * kRow;
           any = false;
+          for (; k < k1; ++k) {
+            const uint32_t off = static_cast<uint32_t>(prog[k]) * kRow;
 #pragma unroll
-          for (int w = 0; w < AW; ++w) {
-            m[w] &= tl[off + 32 * w];
-            any |= m[w] != 0;
+            for (int w = 0; w < AW; ++w) m[w] &= tl[off + 32 * w];
           }
+#pragma unroll
+          for (int w = 0; w < AW; ++w) any |= m[w] != 0;
         }
         const uint32_t word = __ballot_sync(0xFFFFFFFFu, any);
         alive &= word;
