@@ -407,10 +407,11 @@ int launch_graph_derive(Graph* g) {
     k_node_graph<<<grid_for(g->num_graphs, B, 65535u), B, 0, q->stream>>>(g->graph_offsets, g->num_graphs, g->node_graph);
     SIGMO_TRY(check_launch(q, "k_node_graph"));
   }
-  uint32_t mx = g->max_nodes;
-  uint32_t aw = (mx + 63u) / 64u;
-  if (aw < 1) aw = 1;
-  if (aw > kMaxAdjWords) aw = kMaxAdjWords;
+  // words per local adjacency row: 1, 2 or 4 (the kernels are instantiated
+  // for those widths; a batch whose largest graph has 129-192 vertices gets 4)
+  const uint32_t mx = g->max_nodes;
+  uint32_t aw = 1;
+  while (aw < kMaxAdjWords && aw * 64u < mx) aw *= 2;
   g->adj_words = aw;
   const uint64_t adj_elems = g->total_nodes * aw;
   SIGMO_TRY(dev_alloc(q, reinterpret_cast<void**>(&g->adj), sizeof(uint64_t) * (adj_elems ? adj_elems : 1)));

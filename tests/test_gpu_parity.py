@@ -441,17 +441,49 @@ def test_shards_keep_the_unsharded_results(ff):
 
 
 @pytest.mark.gpu
+def _batch_planes(q, R):
+    """The candidate planes of a query batch: its distinct labels and
+    (iteration, label, count) thresholds."""
+    sig = oracle.generate_signatures(q)
+    reach = oracle.new_reach(len(sig), oracle.REF_PTX)
+    thresholds = set()
+    for r in range(1, R + 1):
+        sig = oracle.refine_signatures(q, r, oracle.REF_PTX, sig, reach)
+        for v in sig.tolist():
+            thresholds.update((r, l, (v >> (4 * l)) & 15) for l in range(16) if (v >> (4 * l)) & 15)
+    return len(thresholds) + len(set(oracle.as_batch(q).node_labels.tolist()))
+
+
 def test_query_batch_admitted_in_groups():
-    """A query batch whose planes and classes exceed one admission tile
-    (1,000 queries of 3-40 atoms: ~17k classes; molecules up to 120 atoms,
-    two words per vertex set) is admitted group by group into one plane
-    array; GMCR and per-pair counts equal the oracle's."""
+    """A query batch whose candidate planes exceed one admission tile's
+    shared-memory budget of 96 KB (2,000 queries of 3-64 atoms, 6 iterations:
+    about 200 planes; molecules up to 107 atoms, so every vertex set is two
+    words and a plane row of a 32-graph tile is 512 B) is admitted group by
+    group into one plane array; GMCR and per-pair counts equal the oracle's."""
     d = sb.generate_molecules(1500, 6, 120, seed=4903, kind=1, median=22.0)
-    q = sb.generate_queries(1000, 3, 40, seed=4901)
-    assert d.sizes().max() > 64
-    ref = _oracle(q, d, 4, oracle.REF_PTX, False)
-    got = run_both_batched(q, d, 4, oracle.REF_PTX, False)
+    q = sb.generate_queries(2000, 3, 64, seed=4901)
+    R = 6
+    assert 64 < d.sizes().max() <= 128  # two words per vertex set
+    assert _batch_planes(q, R) * 2 * 32 * 8 > 96 * 1024  # more than one tile: the batch is split into groups
+    ref = _oracle(q, d, R, oracle.REF_PTX, False)
+    got = run_both_batched(q, d, R, oracle.REF_PTX, False)
     _check(got, ref, "grouped admission")
+
+
+@pytest.mark.parametrize("prof", DEVICE_PROFILES)
+def test_molecules_of_129_to_192_atoms(prof):
+    """A batch whose largest molecule has 129-192 atoms (146 here): every
+    local vertex set takes four words (the width the kernels are built for),
+    through the stage-per-launch and batched forms, with planes of four words
+    split into admission groups; everything equals the oracle."""
+    d = sb.generate_molecules(1500, 6, 250, seed=4903, kind=1, median=30.0)
+    q = sb.generate_queries(1000, 3, 40, seed=4901)
+    R = 6
+    assert 128 < d.sizes().max() <= 192
+    assert _batch_planes(q, R) * 4 * 32 * 8 > 96 * 1024  # four-word planes: more than one tile
+    ref = _oracle(q, d, R, prof, False)
+    _check(run_both_batched(q, d, R, prof, False), ref, "batched")
+    _check(run_plain(q, d, R, prof, False), ref, "plain")
 
 
 @pytest.mark.parametrize("prof", (oracle.REF_PTX, oracle.REF_X86))
