@@ -316,6 +316,7 @@ int plan_groups(Queue* q, Graph* query, uint32_t AW, const std::vector<uint32_t>
     }
     r_begin[R] = static_cast<uint32_t>(spec.size());
     for (int r = static_cast<int>(R) - 1; r >= 0; --r) r_begin[r] = std::min(r_begin[r], r_begin[r + 1]);
+    // local programs; qc: per query entry, its class's local program range
     std::vector<uint32_t> loc_class(C, 0xFFFFFFFFu), prog_off{0}, qc_off{0}, qc;
     std::vector<uint16_t> prog;
     for (uint32_t qg = grp.q0; qg < grp.q1; ++qg) {
@@ -327,21 +328,23 @@ int plan_groups(Queue* q, Graph* query, uint32_t AW, const std::vector<uint32_t>
             prog.push_back(static_cast<uint16_t>(loc_plane[pp.h_prog[i]]));
           prog_off.push_back(static_cast<uint32_t>(prog.size()));
         }
-        qc.push_back(loc_class[c]);
+        qc.push_back(prog_off[loc_class[c]]);
+        qc.push_back(prog_off[loc_class[c] + 1]);
       }
-      qc_off.push_back(static_cast<uint32_t>(qc.size()));
+      qc_off.push_back(static_cast<uint32_t>(qc.size() / 2));
     }
     grp.K = static_cast<uint32_t>(spec.size());
     grp.C = static_cast<uint32_t>(prog_off.size() - 1);
-    // every local id the kernel will index with must be inside its array
+    // every local id and range the kernel will index with must be inside its array
     for (uint16_t k : prog)
       if (k >= grp.K) return fail(SIGMO_ERR_INVALID, "internal: group %zu plane %u outside its %u planes", gi, k, grp.K);
-    for (uint32_t c : qc)
-      if (c >= grp.C) return fail(SIGMO_ERR_INVALID, "internal: group %zu class %u outside its %u classes", gi, c, grp.C);
+    for (size_t i = 0; i < qc.size(); i += 2)
+      if (qc[i] > qc[i + 1] || qc[i + 1] > prog.size())
+        return fail(SIGMO_ERR_INVALID, "internal: group %zu program range outside its %zu entries", gi, prog.size());
     if (planes_admit_smem(grp.K, AW) > 200u * 1024u)
       return fail(SIGMO_ERR_DOMAIN, "group %zu needs more than one admission tile of shared memory", gi);
     grp.nlab = nlab;
-    grp.n_qc = qc.size();
+    grp.n_qc = qc.size() / 2;
     grp.n_prog = prog.size();
     SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.spec), spec.data(), 4 * spec.size()));
     SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.r_begin), r_begin.data(), 4 * r_begin.size()));
@@ -392,8 +395,14 @@ int order_classes(Queue* q, Graph* query, Graph* data) {
   dev_free(q, pp.qc_off);
   dev_free(q, pp.qc);
   pp.qc_off = pp.qc = nullptr;
+  // the kernel reads each entry as its class's program range [begin, end) in prog
+  std::vector<uint32_t> ranges(2 * list.size());
+  for (size_t e = 0; e < list.size(); ++e) {
+    ranges[2 * e] = pp.h_prog_off[list[e]];
+    ranges[2 * e + 1] = pp.h_prog_off[list[e] + 1];
+  }
   SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.qc_off), off.data(), 4 * off.size()));
-  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.qc), list.data(), 4 * list.size()));
+  SIGMO_TRY(upload(q, reinterpret_cast<void**>(&pp.qc), ranges.data(), 4 * ranges.size()));
   pp.h_qc_n = list.size();
   free_groups(q, &pp);
   const uint32_t AW = data->adj_words;

@@ -95,7 +95,7 @@ struct PlaneGroup {
   uint32_t* prog_off = nullptr;  // [C + 1]
   uint16_t* prog = nullptr;      // local plane ids
   uint32_t* qc_off = nullptr;    // [q1 - q0 + 1]
-  uint32_t* qc = nullptr;        // local class ids in evaluation order
+  uint32_t* qc = nullptr;        // per entry in evaluation order, its local program range (begin, end)
   size_t n_qc = 0, n_prog = 0;
 };
 
@@ -119,7 +119,7 @@ struct PlaneProgram {
   // per query graph, its distinct classes in evaluation order for one data
   // graph's label frequencies (rebuilt when the data graph changes)
   uint32_t* qc_off = nullptr;     // [query graphs + 1]
-  uint32_t* qc = nullptr;
+  uint32_t* qc = nullptr;         // per entry, its class's program range in prog: (begin, end) u32 pairs
   size_t h_qc_n = 0;              // entries of qc
   std::vector<PlaneGroup> groups; // empty: the whole batch fits one tile
   const void* qc_for = nullptr;   // the data graph the order was built for

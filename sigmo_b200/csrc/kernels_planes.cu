@@ -166,7 +166,7 @@ __device__ __forceinline__ void gather_tile_async(uint64_t* dst, const uint64_t*
 // Shared-memory layout of k_planes_admit (in u64 units for the tiles):
 //   tile buffer(s) [1 or 2][K * AW * 32] u64, s_map[K] (gather), then the
 //   staged class lists when they fit:
-//   qc_off[QG + 1], qc[n_qc], prog_off[C + 1] (u32), prog[n_prog] (u16).
+//   qc[n_qc] (uint2 program ranges), qc_off[QG + 1] (u32), prog[n_prog] (u16).
 struct AdmitSmem {
   size_t tiles, map, lists, total;
 };
@@ -189,8 +189,8 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
     int prof, uint32_t base, const uint64_t* __restrict__ rplanes, uint32_t rrows, const uint32_t* __restrict__ row_map,
     uint32_t QG,
-    const uint32_t* __restrict__ qgoff, uint32_t C, const uint32_t* __restrict__ g_prog_off, const uint16_t* __restrict__ g_prog,
-    const uint32_t* __restrict__ g_qc_off, const uint32_t* __restrict__ g_qc, uint32_t n_qc, uint32_t n_prog, int stage_lists,
+    const uint32_t* __restrict__ qgoff, const uint16_t* __restrict__ g_prog, const uint32_t* __restrict__ g_qc_off,
+    const uint2* __restrict__ g_qc, uint32_t n_qc, uint32_t n_prog, int stage_lists,
     const uint32_t* __restrict__ row_of, uint32_t out_rows, int accumulate, uint64_t* __restrict__ planes,
     uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -199,27 +199,25 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t GW = (G + 31u) / 32u;
   const uint32_t words = K * AW;
-  const size_t list_bytes = stage_lists ? 4ull * (QG + 1 + n_qc + C + 1) + 2ull * n_prog : 0;
+  const size_t list_bytes = stage_lists ? 8ull * n_qc + 4ull * (QG + 1) + 2ull * n_prog : 0;
   const AdmitSmem L = admit_smem_layout(K, AW, GATHER, list_bytes);
   uint64_t* tiles = reinterpret_cast<uint64_t*>(smem_raw);
   uint32_t* s_map = reinterpret_cast<uint32_t*>(smem_raw + L.map);
   // per-batch constants: the row map and (when they fit) the class lists
   const uint32_t* qc_off = g_qc_off;
-  const uint32_t* qc = g_qc;
-  const uint32_t* prog_off = g_prog_off;
+  const uint2* qc = g_qc;
   const uint16_t* prog = g_prog;
   if (GATHER)
     for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) s_map[i] = row_map[i];
   if (stage_lists) {
-    uint32_t* p = reinterpret_cast<uint32_t*>(smem_raw + L.lists);
+    uint2* p2 = reinterpret_cast<uint2*>(smem_raw + L.lists);
+    for (uint32_t i = threadIdx.x; i < n_qc; i += blockDim.x) p2[i] = g_qc[i];
+    uint32_t* p = reinterpret_cast<uint32_t*>(p2 + n_qc);
     for (uint32_t i = threadIdx.x; i <= QG; i += blockDim.x) p[i] = g_qc_off[i];
-    for (uint32_t i = threadIdx.x; i < n_qc; i += blockDim.x) p[QG + 1 + i] = g_qc[i];
-    for (uint32_t i = threadIdx.x; i <= C; i += blockDim.x) p[QG + 1 + n_qc + i] = g_prog_off[i];
-    uint16_t* p16 = reinterpret_cast<uint16_t*>(p + QG + 1 + n_qc + C + 1);
+    uint16_t* p16 = reinterpret_cast<uint16_t*>(p + QG + 1);
     for (uint32_t i = threadIdx.x; i < n_prog; i += blockDim.x) p16[i] = g_prog[i];
+    qc = p2;
     qc_off = p;
-    qc = p + QG + 1;
-    prog_off = p + QG + 1 + n_qc;
     prog = p16;
   }
   __syncthreads();
@@ -261,14 +259,14 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
       uint32_t alive = qgoff[qg + 1] - qgoff[qg] > 1u ? valid_lanes : 0u;
       const uint32_t e1 = qc_off[qg + 1];
       for (uint32_t e = qc_off[qg]; e < e1 && alive; ++e) {
-        const uint32_t c = qc[e];
+        const uint2 pr = qc[e];  // the class's program: prog[pr.x, pr.y)
         uint64_t m[AW];
 #pragma unroll
         for (int w = 0; w < AW; ++w) m[w] = ~0ull;
         bool any = true;
-        const uint32_t k1 = prog_off[c + 1];
+        const uint32_t k1 = pr.y;
         // four planes per step between the warp votes
-        uint32_t k = prog_off[c];
+        uint32_t k = pr.x;
         bool live = true;
         for (; k + 4 <= k1; k += 4) {
           const uint32_t off0 = static_cast<uint32_t>(prog[k]) * kRow, off1 = static_cast<uint32_t>(prog[k + 1]) * kRow;
@@ -408,7 +406,7 @@ int admit_launch(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t 
                  uint32_t rrows, const uint32_t* row_map, uint64_t* planes, uint32_t* admit, uint32_t* counts) {
   const uint32_t G = data->num_graphs, GW = (G + 31u) / 32u, QG = v.QG;
   const uint32_t n_qc = static_cast<uint32_t>(v.n_qc), n_prog = static_cast<uint32_t>(v.n_prog);
-  const size_t list_bytes = 4ull * (QG + 1 + n_qc + v.C + 1) + 2ull * n_prog;
+  const size_t list_bytes = 8ull * n_qc + 4ull * (QG + 1) + 2ull * n_prog;
   const size_t base = admit_smem_layout(v.K, AW, GATHER, 0).total;
   // stage the class lists when the block still fits three to an SM
   const int stage = base + list_bytes <= 72u * 1024u ? 1 : 0;
@@ -423,7 +421,8 @@ int admit_launch(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t 
   const uint64_t grid = std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms);
   k_planes_admit<AW, GATHER><<<grid, block, smem, q->stream>>>(
       G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, v.K, v.nlab, v.spec, v.r_begin, q->opts.profile,
-      data->vertex_base, rplanes, rrows, row_map, QG, v.qgoff, v.C, v.prog_off, v.prog, v.qc_off, v.qc, n_qc, n_prog, stage,
+      data->vertex_base, rplanes, rrows, row_map, QG, v.qgoff, v.prog, v.qc_off, reinterpret_cast<const uint2*>(v.qc), n_qc,
+      n_prog, stage,
       v.row_of, v.out_rows, v.accumulate, planes, admit, counts);
   return check_launch(q, "k_planes_admit");
 }
