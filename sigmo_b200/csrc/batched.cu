@@ -381,6 +381,9 @@ int order_classes(Queue* q, Graph* query, Graph* data) {
   parallel_ranges(QG, host_threads(query->total_nodes), [&](unsigned, uint64_t q0, uint64_t q1) {
     for (uint64_t qg = q0; qg < q1; ++qg) {
       std::vector<uint32_t>& tmp = per[qg];
+      // queries of one vertex are never admitted (gmcr.hpp:100): an empty list
+      // tells the kernel so
+      if (pp.h_qgoff[qg + 1] - pp.h_qgoff[qg] <= 1) continue;
       tmp.assign(pp.h_cls.begin() + pp.h_qgoff[qg], pp.h_cls.begin() + pp.h_qgoff[qg + 1]);
       std::sort(tmp.begin(), tmp.end());
       tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());

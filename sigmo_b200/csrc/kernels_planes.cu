@@ -108,7 +108,8 @@ __device__ __forceinline__ void build_graph_planes(uint64_t* tile, uint32_t gl, 
 // between queries, and without a per-class cache in shared memory four CTAs
 // fit on an SM instead of three.  The per-graph admitted counts (the GMCR
 // segment lengths) are summed in shared memory.  Queries of one vertex are
-// never admitted (the reference's mapping skips them, gmcr.hpp:100).
+// never admitted (the reference's mapping skips them, gmcr.hpp:100): their
+// class lists are empty.
 constexpr uint32_t kAdmitWarps = 16;
 
 // The tile's planes: built from the data signatures (and written out for the
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     uint64_t N, uint32_t R, uint32_t K, uint32_t nlab, const uint32_t* __restrict__ spec, const uint32_t* __restrict__ r_begin,
     int prof, uint32_t base, const uint64_t* __restrict__ rplanes, uint32_t rrows, const uint32_t* __restrict__ row_map,
     uint32_t QG,
-    const uint32_t* __restrict__ qgoff, const uint16_t* __restrict__ g_prog, const uint32_t* __restrict__ g_qc_off,
+    const uint16_t* __restrict__ g_prog, const uint32_t* __restrict__ g_qc_off,
     const uint2* __restrict__ g_qc, uint32_t n_qc, uint32_t n_prog, int stage_lists,
     const uint32_t* __restrict__ row_of, uint32_t out_rows, int accumulate, uint64_t* __restrict__ planes,
     uint32_t* __restrict__ admit, uint32_t* __restrict__ counts) {
@@ -256,9 +257,9 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     const uint32_t valid_lanes = in_tile >= 32u ? 0xFFFFFFFFu : ((1u << in_tile) - 1u);
     uint32_t my_cnt = 0;
     for (uint32_t qg = wid; qg < QG; qg += nw) {
-      uint32_t alive = qgoff[qg + 1] - qgoff[qg] > 1u ? valid_lanes : 0u;
-      const uint32_t e1 = qc_off[qg + 1];
-      for (uint32_t e = qc_off[qg]; e < e1 && alive; ++e) {
+      const uint32_t e0 = qc_off[qg], e1 = qc_off[qg + 1];
+      uint32_t alive = e1 > e0 ? valid_lanes : 0u;  // an empty list: a query of at most one vertex
+      for (uint32_t e = e0; e < e1 && alive; ++e) {
         const uint2 pr = qc[e];  // the class's program: prog[pr.x, pr.y)
         uint64_t m[AW];
 #pragma unroll
@@ -421,7 +422,7 @@ int admit_launch(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t 
   const uint64_t grid = std::min<uint64_t>(GW, static_cast<uint64_t>(std::max(per_sm, 1)) * sms);
   k_planes_admit<AW, GATHER><<<grid, block, smem, q->stream>>>(
       G, data->graph_offsets, data->node_labels, sig_all, data->total_nodes, R, v.K, v.nlab, v.spec, v.r_begin, q->opts.profile,
-      data->vertex_base, rplanes, rrows, row_map, QG, v.qgoff, v.prog, v.qc_off, reinterpret_cast<const uint2*>(v.qc), n_qc,
+      data->vertex_base, rplanes, rrows, row_map, QG, v.prog, v.qc_off, reinterpret_cast<const uint2*>(v.qc), n_qc,
       n_prog, stage,
       v.row_of, v.out_rows, v.accumulate, planes, admit, counts);
   return check_launch(q, "k_planes_admit");
