@@ -165,7 +165,7 @@ __device__ __forceinline__ void gather_tile_async(uint64_t* dst, const uint64_t*
 }
 
 // Shared-memory layout of k_planes_admit (in u64 units for the tiles):
-//   tile buffer(s) [1 or 2][K * AW * 32] u64, s_map[K] (gather), then the
+//   tile buffer [K * AW * 32] u64, s_map[K] (gather), then the
 //   staged class lists when they fit:
 //   qc[n_qc] (uint2 program ranges), qc_off[QG + 1] (u32), prog[n_prog] (u16).
 struct AdmitSmem {
@@ -174,7 +174,7 @@ struct AdmitSmem {
 __host__ __device__ inline AdmitSmem admit_smem_layout(uint32_t K, uint32_t AW, bool gather, size_t list_bytes) {
   AdmitSmem l{};
   l.tiles = 0;
-  size_t off = static_cast<size_t>(gather ? 2 : 1) * K * AW * 32 * 8;
+  size_t off = static_cast<size_t>(K) * AW * 32 * 8;
   l.map = off;
   off += gather ? 4ull * K : 0;
   off = (off + 15) & ~static_cast<size_t>(15);
@@ -222,15 +222,14 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
     prog = p16;
   }
   __syncthreads();
-  uint32_t buf = 0;
-  if (GATHER && blockIdx.x < GW) gather_tile_async<AW>(tiles, rplanes, rrows, blockIdx.x, K, s_map);
   for (uint32_t gw = blockIdx.x; gw < GW; gw += gridDim.x) {
-    uint64_t* tile = tiles + static_cast<size_t>(buf) * words * 32;
+    uint64_t* tile = tiles;
     if (GATHER) {
-      cp_async_wait_all();
-      __syncthreads();  // this tile has landed; every warp is done with the previous one
-      const uint32_t next = gw + gridDim.x;
-      if (next < GW) gather_tile_async<AW>(tiles + static_cast<size_t>(buf ^ 1u) * words * 32, rplanes, rrows, next, K, s_map);
+      // one tile buffer (not two, double-buffered): at 35 KB instead of 70 KB
+      // per CTA more CTAs share an SM and hide each other's gathers
+      __syncthreads();  // every warp is done with the previous tile
+      gather_tile_async<AW>(tile, rplanes, rrows, gw, K, s_map);
+      cp_async_wait_all();  // this thread's copies; the barrier below covers the others'
     } else {
       __syncthreads();  // the previous tile is no longer read
       fill_tile<AW, false>(tile, gw, G, goff, lab, sig_all, N, R, K, nlab, spec, r_begin, prof, base, nullptr, 0, nullptr);
@@ -305,7 +304,6 @@ __global__ void __launch_bounds__(kAdmitWarps * 32) k_planes_admit(
       if (accumulate) atomicAdd(&counts[gw * 32u + threadIdx.x], tile_cnt[threadIdx.x]);
       else counts[gw * 32u + threadIdx.x] = tile_cnt[threadIdx.x];
     }
-    buf ^= GATHER ? 1u : 0u;
   }
   if (GATHER) cp_async_wait_all();
 }
