@@ -20,7 +20,6 @@ void free_groups(Queue* q, PlaneProgram* pp) {
     dev_free(q, g.spec);
     dev_free(q, g.r_begin);
     dev_free(q, g.row_of);
-    dev_free(q, g.prog_off);
     dev_free(q, g.prog);
     dev_free(q, g.qc_off);
     dev_free(q, g.qc);
@@ -349,7 +348,6 @@ int plan_groups(Queue* q, Graph* query, uint32_t AW, const std::vector<uint32_t>
     SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.spec), spec.data(), 4 * spec.size()));
     SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.r_begin), r_begin.data(), 4 * r_begin.size()));
     SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.row_of), row_of.data(), 4 * row_of.size()));
-    SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.prog_off), prog_off.data(), 4 * prog_off.size()));
     SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.prog), prog.data(), 2 * prog.size()));
     SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.qc_off), qc_off.data(), 4 * qc_off.size()));
     SIGMO_TRY(upload(q, reinterpret_cast<void**>(&grp.qc), qc.data(), 4 * qc.size()));

@@ -82,18 +82,17 @@ int join_status_reset(Queue* q);
 int join_status_fetch(Queue* q);
 int join_status_result(Queue* q);
 
-// A contiguous range of query graphs whose planes and classes fit one
-// k_planes_admit tile in shared memory (a batch too large for one tile is
-// admitted group by group).  Device arrays are in group-local plane and class
-// ids; row_of maps a local plane to its row in the batch's plane array.
+// A contiguous range of query graphs whose planes fit one k_planes_admit
+// tile in shared memory (a batch too large for one tile is admitted group by
+// group).  Device arrays are in group-local plane ids; row_of maps a local
+// plane to its row in the batch's plane array.
 struct PlaneGroup {
   uint32_t q0 = 0, q1 = 0;
   uint32_t K = 0, C = 0, nlab = 0;
   uint32_t* spec = nullptr;      // [K]
   uint32_t* r_begin = nullptr;   // [R + 1]
   uint32_t* row_of = nullptr;    // [K] plane row in the batch
-  uint32_t* prog_off = nullptr;  // [C + 1]
-  uint16_t* prog = nullptr;      // local plane ids
+  uint16_t* prog = nullptr;      // the group's class programs, local plane ids
   uint32_t* qc_off = nullptr;    // [q1 - q0 + 1]
   uint32_t* qc = nullptr;        // per entry in evaluation order, its local program range (begin, end)
   size_t n_qc = 0, n_prog = 0;

@@ -392,8 +392,11 @@ namespace {
 // What one admission launch needs of a program: the whole batch's, or one
 // group's (local ids; planes scattered to row_of).
 struct AdmitView {
-  uint32_t K, C, nlab, QG;
-  const uint32_t *spec, *r_begin, *prog_off, *qc_off, *qc, *qgoff, *row_of;
+  uint32_t K, nlab, QG;
+  const uint32_t *spec, *r_begin;
+  const uint32_t* qc_off;  // [QG + 1] entries of qc per query graph
+  const uint32_t* qc;      // per entry, its class's program range in prog (u32 pairs)
+  const uint32_t* row_of;  // group launches: local plane row -> row of the batch's plane array
   const uint16_t* prog;
   size_t n_qc, n_prog;
   uint32_t out_rows;
@@ -427,9 +430,8 @@ int admit_launch(Queue* q, const Graph* data, const uint64_t* sig_all, uint32_t 
 }
 
 AdmitView whole_batch(const Graph* query, const PlaneProgram& pp) {
-  return AdmitView{pp.K,      pp.C,       pp.nlab,  query->num_graphs, pp.spec, pp.r_begin, pp.prog_off,
-                   pp.qc_off, pp.qc,      query->graph_offsets, nullptr, pp.prog, pp.h_qc_n, pp.h_prog.size(),
-                   pp.K,      0};
+  return AdmitView{pp.K, pp.nlab, query->num_graphs, pp.spec, pp.r_begin, pp.qc_off, pp.qc, nullptr, pp.prog, pp.h_qc_n,
+                   pp.h_prog.size(), pp.K, 0};
 }
 
 }  // namespace
@@ -449,9 +451,8 @@ int launch_planes_admit_group(Queue* q, const Graph* query, const Graph* data, c
                               const PlaneGroup& grp, uint32_t K_total, uint64_t* planes, uint32_t* admit, uint32_t* counts) {
   if (!data->num_graphs || grp.q1 <= grp.q0) return SIGMO_OK;
   const uint32_t GW = (data->num_graphs + 31u) / 32u;
-  const AdmitView v{grp.K,      grp.C,  grp.nlab, grp.q1 - grp.q0, grp.spec, grp.r_begin, grp.prog_off,
-                    grp.qc_off, grp.qc, query->graph_offsets + grp.q0, grp.row_of, grp.prog, grp.n_qc, grp.n_prog,
-                    K_total,    1};
+  const AdmitView v{grp.K,      grp.nlab, grp.q1 - grp.q0, grp.spec, grp.r_begin, grp.qc_off, grp.qc, grp.row_of, grp.prog,
+                    grp.n_qc, grp.n_prog, K_total, 1};
   uint32_t* adm = admit + static_cast<uint64_t>(grp.q0) * GW;
   switch (data->adj_words) {
     case 1: return admit_launch<1, false>(q, data, sig_all, R, v, nullptr, 0, nullptr, planes, adm, counts);
